@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: particle-substeps per second of the explicit MPM substep on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+A step is one substep (binning, P2G, grid update with explicit phase field,
+G2P with SVD + return map) of the whole scene.  Default workload: 4 stacked
+plates of 256x256x16 cells at dx=1/256, 8 particles per cell (33,554,432
+particles), sphere impactor r=0.1 at 5 m/s, gravity -9.8, dt=5e-5, FP32,
+deterministic P2G.  Synthetic seeded data (the reference's sampled assets are
+not shipped).  The resident state (about 9 GB) is far larger than L2.
+
+With N>1 (torchrun, one process per GPU) every rank advances its own replica
+of the scene: the path has no exchange step, scaling is weak and `value` is
+the sum over ranks, timed as the max over ranks.
+
+`--impl reference` times the oracle (the FP64 CPU restatement of the
+reference's algorithm; the reference itself has no CPU path) on the host
+cores, on a bounded sample of the same workload (4 plates of 48x48x16 cells,
+same dx, ppc and materials).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "explicit-gpumpm-ductile-fracture_b200"
+
+# Algorithmic bytes (FP32 state layout; one read or write of each byte the
+# kernel must touch).  Per particle / per grid node of a grid page.
+ALGO_BYTES = {
+    "sort": dict(particle=20, node=0),    # read x (12) + write key and slot (8)
+    "p2g": dict(particle=112, node=36),   # read x v B sigma c m V FP q; write 9 channels per node
+    "grid": dict(particle=0, node=56),    # read 9 channels, write 5 channels per node
+    "g2p": dict(particle=224, node=20),   # read x F c alpha psi m id; write x v F B c alpha psi sigma V FP q m id
+}
+STAGE_KEY = {"sort": "bin_ms", "p2g": "p2g_ms", "grid": "grid_ms", "g2p": "g2p_ms"}
+CPU_SAMPLE_CELLS = 48
+
+
+def load_package():
+    spec = importlib.util.spec_from_file_location("gmpm_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["gmpm_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle  # noqa: E402  (test/baseline infrastructure)
+    oracle.build()
+    return oracle
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
+    return dict(hbm_gbs=6650.0, source="fallback")
+
+
+def measured_traffic() -> dict:
+    """DRAM bytes per particle per kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic_per_particle.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+def workload(pkg, name: str, seed: int = 0):
+    S = pkg.scenes
+    if name == "plates_33m":
+        return S.plates(seed=seed), ("plates_33m: 4 plates of 256x256x16 cells, dx=1/256, 8 ppc, "
+                                     "sphere impactor r=0.1 at 5 m/s, g=-9.8, dt=5e-5")
+    if name == "plates_8m":
+        return S.plates_8m(seed=seed), ("plates_8m: 4 plates of 128x128x16 cells, dx=1/128, 8 ppc, "
+                                        "sphere impactor r=0.1 at 5 m/s, g=-9.8, dt=5e-5")
+    if name == "notched_bar":
+        return S.notched_bar(seed=seed), ("notched_bar: 16x16x64 cells, dx=1/128, 8 ppc, pulled at +/-0.5 m/s, "
+                                          "dt=1e-4")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_sample(pkg, name: str):
+    S = pkg.scenes
+    if name.startswith("plates"):
+        dx = 1.0 / 256 if name == "plates_33m" else 1.0 / 128
+        sp = S._plate_scene("plates_sample", CPU_SAMPLE_CELLS, dx, 8, 8, 8 if dx < 1 / 200 else 4,
+                            160 if dx < 1 / 200 else 96, 0, pkg.gmpm.PRECISION_FP64, 10)
+        return sp, f"4 plates of {CPU_SAMPLE_CELLS}x{CPU_SAMPLE_CELLS}x16 cells (same dx, ppc, materials), {sp.n} particles"
+    sp = S.notched_bar(precision=pkg.gmpm.PRECISION_FP64)
+    return sp, f"the full notched bar, {sp.n} particles"
+
+
+def time_oracle(pkg, oracle, name: str, steps: int, warmup: int, budget_s: float | None = None):
+    sp, what = cpu_sample(pkg, name)
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    o = oracle.OracleScene(sp.desc, sp.positions, sp.masses, sp.velocities, sp.material_ids)
+    o.substep(max(0, warmup))
+    per = []
+    t_all = time.perf_counter()
+    for _ in range(steps):
+        t = time.perf_counter()
+        o.substep(1)
+        per.append(time.perf_counter() - t)
+        if budget_s is not None and time.perf_counter() - t_all > budget_s:
+            break
+    total = sum(per)
+    return dict(value=sp.n * len(per) / total, unit="particle-substeps/s", cores=oracle.get_threads(),
+                kind="port", sample=f"{what}; {len(per)} substeps after {warmup} warm-up",
+                ms_per_step=1e3 * total / len(per))
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, which: str):
+        setattr(self, which, time.time())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
+        # samples inside the timed region (plus the one straddling its start)
+        inside = [l for t, l in self.lines if t0 - 0.2 <= t <= t1 + 0.05]
+        for l in inside:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=mx, reasons=sorted(reasons),
+                    samples=len(sm))
+
+
+def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
+    import torch
+
+    G = pkg.gmpm
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = G.Context(local_rank)
+    sp, what = workload(pkg, args.workload)
+    t0 = time.perf_counter()
+    scene = sp.build(ctx)
+    build_s = time.perf_counter() - t0
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    scene.substep(args.warmup, sh)
+    torch.cuda.synchronize(dev)
+    launches0 = scene.diagnostics()["kernel_launches"]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        torch.cuda.synchronize(dev)
+        clocks.mark("t0")
+        start.record(stream)
+        scene.substep(args.steps, sh)
+        end.record(stream)
+        end.synchronize()
+        clocks.mark("t1")
+        torch.cuda.synchronize(dev)
+        barrier()
+    ms = start.elapsed_time(end)
+    diag = scene.diagnostics()
+    launches = diag["kernel_launches"] - launches0
+    status = scene.sync()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * sp.n * args.steps / (ms_max / 1e3)
+
+    # per-stage device times (CUDA events on the same stream) for the roofline
+    stages = scene.substep_timed(min(5, max(1, args.steps)), sh)
+    nsub = max(1, stages["substeps"])
+    nodes = 64 * diag["n_grid_blocks"]
+    peaks = measured_peaks()
+    traffic = measured_traffic()
+    kernels = {}
+    for k, key in STAGE_KEY.items():
+        t = stages[key] / nsub / 1e3
+        b = ALGO_BYTES[k]["particle"] * sp.n + ALGO_BYTES[k]["node"] * nodes
+        gbs = b / t / 1e9 if t > 0 else 0.0
+        tr = traffic.get(k)
+        kernels[k] = dict(ms=round(t * 1e3, 4), algo_bytes=b, achieved_gbs=round(gbs, 1),
+                          frac=round(gbs / peaks["hbm_gbs"], 4),
+                          traffic=(int(tr * sp.n) if tr is not None else None))
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+
+    # end to end through the C-ABI, the reference's frame loop: host-set velocity
+    # conditions (H2D), one substep, positions + damage back to pinned host memory (D2H).
+    e2e = None
+    if not args.no_e2e:
+        pos_h = torch.empty(sp.n * 3, dtype=torch.float32, pin_memory=True)
+        dmg_h = torch.empty(sp.n, dtype=torch.float32, pin_memory=True)
+        nsph = sp.desc.n_sphere_bcs
+        nslab = sp.desc.n_slab_bcs
+        sph_h = torch.empty(max(1, nsph) * 56, dtype=torch.uint8, pin_memory=True)
+        slab_h = torch.empty(max(1, nslab) * 48, dtype=torch.uint8, pin_memory=True)
+        import ctypes as C
+        C.memmove(sph_h.data_ptr(), C.addressof(sp.desc.spheres), max(1, nsph) * 56)
+        C.memmove(slab_h.data_ptr(), C.addressof(sp.desc.slabs), max(1, nslab) * 48)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            scene.set_velocity_conditions_raw(slab_h.data_ptr(), nslab, sph_h.data_ptr(), nsph, sh)
+            scene.substep(1, sh)
+            scene.read_into("position", pos_h.data_ptr(), pos_h.numel() * 4, order=G.ORDER_INTERNAL,
+                            dtype=G.DTYPE_F32, stream=sh)
+            scene.read_into("damage", dmg_h.data_ptr(), dmg_h.numel() * 4, order=G.ORDER_INTERNAL,
+                            dtype=G.DTYPE_F32, stream=sh)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        e_ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
+        e_ms = float(e_ms.item())
+        bc_bytes = sizeof_velocity_conditions(np.float32)
+        e2e = dict(value=world * sp.n * args.steps / (e_ms / 1e3), unit="particle-substeps/s",
+                   h2d_bytes_per_step=bc_bytes, d2h_bytes_per_step=sp.n * 16,
+                   note="per step: velocity conditions H2D (pinned), gmpm_substep, positions+damage FP32 D2H "
+                        "(pinned) through the C-ABI, as MPMSimulator::simulateStick + Attribs_Back_Host")
+    return dict(sp=sp, what=what, value=value, ms_max=ms_max, launches=launches, clocks=clocks.summary(),
+                kernels=kernels, dom=dom, peaks=peaks, e2e=e2e, status=status, build_s=build_s, diag=diag)
+
+
+def sizeof_velocity_conditions(dt) -> int:
+    # int n_slabs, n_spheres, slab_axis[4]; Real lo[4], hi[4], vel[4][3], c[2][3], r[2], v[2][3]
+    r = np.dtype(dt).itemsize
+    ints = 4 * (2 + 4)
+    reals = r * (4 + 4 + 12 + 6 + 2 + 6)
+    return ints + reals
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="plates_33m", choices=["plates_33m", "plates_8m", "notched_bar"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    pkg = load_package()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        oracle = load_oracle()
+        r = time_oracle(pkg, oracle, args.workload, args.steps, args.warmup)
+        sp, what = workload(pkg, args.workload)
+        line = dict(metric="particle-substeps/sec", value=r["value"], unit="particle-substeps/s", n_gpus=0,
+                    steps=args.steps, warmup=args.warmup, ms_per_step=r["ms_per_step"], higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                    config=dict(workload=what, sample=r["sample"]), impl="reference",
+                    cpu_baseline=dict(value=r["value"], unit=r["unit"], cores=r["cores"], kind=r["kind"],
+                                      sample=r["sample"]),
+                    e2e=dict(value=r["value"], unit=r["unit"], h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+        print(json.dumps(line))
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        res = run_ours(args, pkg, rank, local_rank, world, dist)
+    finally:
+        pass
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        oracle = load_oracle()
+        r = time_oracle(pkg, oracle, args.workload, steps=50, warmup=1, budget_s=20.0)
+        cpu = dict(value=r["value"], unit=r["unit"], cores=r["cores"], kind=r["kind"], sample=r["sample"])
+    if rank == 0:
+        sp = res["sp"]
+        k = res["kernels"][res["dom"]]
+        line = dict(
+            metric="particle-substeps/sec", value=res["value"], unit="particle-substeps/s", n_gpus=world,
+            steps=args.steps, warmup=args.warmup, ms_per_step=res["ms_max"] / args.steps, higher_is_better=True,
+            scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+            config=dict(workload=res["what"], particles_per_gpu=sp.n, precision="fp32", deterministic_p2g=True,
+                        parallelism=f"replicas x{world}" if world > 1 else "single scene",
+                        l2="resident state larger than L2 (no flush needed)"),
+            roofline=dict(bound="hbm", kernel=res["dom"], achieved=k["achieved_gbs"], peak=res["peaks"]["hbm_gbs"],
+                          unit="GB/s", frac=k["frac"], traffic=k["traffic"],
+                          peak_source=res["peaks"]["source"]),
+            kernels=res["kernels"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
+            gpu_launches=res["launches"], status=pkg.gmpm.STATUS_NAMES.get(res["status"], res["status"]),
+            n_blocks=res["diag"]["n_blocks"], n_grid_blocks=res["diag"]["n_grid_blocks"])
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,815 @@
+// C-ABI of the substep library (include/gmpm.h): context and scene lifetime,
+// stepping, readback and diagnostics.  Every entry point returns a status;
+// no call exits the process.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "kernels.h"
+
+struct gmpm_context {
+    int device;
+    int num_sms;
+    cudaDeviceProp prop;
+};
+
+namespace gmpm {
+
+namespace {
+
+#define GMPM_TRY(expr)                                   \
+    do {                                                 \
+        cudaError_t e_ = (expr);                         \
+        if (e_ != cudaSuccess) return cuda_status(e_);   \
+    } while (0)
+
+gmpm_status cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return GMPM_OK;
+    if (e == cudaErrorMemoryAllocation) return GMPM_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return GMPM_NO_DEVICE;
+    return GMPM_CUDA_ERROR;
+}
+
+// Gauss-Jordan with the full pivot search of the reference's Inverse()
+// (ExplicitTimeIntegrator.cu:71-129); evaluated once per material on the host.
+void stiffness_inverse(double lambda, double mu, double* D) {
+    double mat[9] = {2 * mu + lambda, lambda, lambda, lambda, 2 * mu + lambda, lambda, lambda, lambda, 2 * mu + lambda};
+    int swapR[3], swapC[3];
+    int pivot[3] = {0, 0, 0};
+    for (int i = 0; i < 3; ++i) {
+        int pr = 0, pc = 0;
+        double maxv = 0;
+        for (int j = 0; j < 3; ++j)
+            if (pivot[j] != 1)
+                for (int k = 0; k < 3; ++k)
+                    if (pivot[k] == 0 && mat[j * 3 + k] > maxv) {
+                        maxv = mat[j * 3 + k];
+                        pr = j;
+                        pc = k;
+                    }
+        if (pr != pc)
+            for (int j = 0; j < 3; ++j) {
+                const double t = mat[pr * 3 + j];
+                mat[pr * 3 + j] = mat[pc * 3 + j];
+                mat[pc * 3 + j] = t;
+            }
+        swapC[i] = pc;
+        swapR[i] = pr;
+        ++pivot[i];
+        const double inv = 1.0 / mat[pc * 3 + pc];
+        mat[pc * 3 + pc] = 1;
+        for (int j = 0; j < 3; ++j) mat[pc * 3 + j] *= inv;
+        for (int j = 0; j < 3; ++j)
+            if (j != pc) {
+                const double ratio = mat[j * 3 + pc];
+                mat[j * 3 + pc] = 0.0;
+                for (int k = 0; k < 3; ++k) mat[j * 3 + k] -= mat[pc * 3 + k] * ratio;
+            }
+    }
+    for (int i = 0; i < 3; ++i)
+        if (swapR[i] != swapC[i])
+            for (int j = 0; j < 3; ++j) {
+                const double t = mat[j * 3 + swapC[i]];
+                mat[j * 3 + swapC[i]] = mat[j * 3 + swapR[i]];
+                mat[j * 3 + swapR[i]] = t;
+            }
+    for (int q = 0; q < 9; ++q) D[q] = mat[q];
+}
+
+template <typename R>
+void fill_velocity_conditions(const gmpm_slab_bc* slabs, int n_slabs, const gmpm_sphere_bc* spheres, int n_spheres,
+                              VelocityConditions<R>& bc) {
+    std::memset(&bc, 0, sizeof(bc));
+    bc.n_slabs = n_slabs;
+    bc.n_spheres = n_spheres;
+    for (int q = 0; q < n_slabs; ++q) {
+        bc.slab_axis[q] = slabs[q].axis;
+        bc.slab_lo[q] = (R)slabs[q].lo;
+        bc.slab_hi[q] = (R)slabs[q].hi;
+        for (int a = 0; a < 3; ++a) bc.slab_vel[q][a] = (R)slabs[q].velocity[a];
+    }
+    for (int q = 0; q < n_spheres; ++q) {
+        for (int a = 0; a < 3; ++a) {
+            bc.sph_c[q][a] = (R)spheres[q].center[a];
+            bc.sph_v[q][a] = (R)spheres[q].velocity[a];
+        }
+        bc.sph_r[q] = (R)spheres[q].radius;
+    }
+}
+
+template <typename R>
+void fill_scene_dev(const gmpm_scene_desc& d, int key_bits, SceneDev<R>& s) {
+    std::memset(&s, 0, sizeof(s));
+    s.dx = (R)d.dx;
+    s.inv_dx = (R)(1.0 / d.dx);
+    s.dt = (R)d.dt;
+    s.Dinv = (R)(4.0 / (d.dx * d.dx));
+    for (int a = 0; a < 3; ++a) {
+        s.gravity[a] = (R)d.gravity[a];
+        s.res[a] = d.grid_res[a];
+    }
+    s.V0 = (R)d.particle_volume;
+    s.key_bits = key_bits;
+    s.n_materials = d.n_materials;
+    for (int m = 0; m < d.n_materials; ++m) {
+        const gmpm_material& in = d.materials[m];
+        MaterialDev<R>& o = s.mat[m];
+        // Lame parameters as ElasticMaterial (Materials.cpp:4-13)
+        const double E = in.youngs_modulus, nu = in.poisson_ratio;
+        const double lambda = E * nu / ((1 + nu) * (1 - 2 * nu));
+        const double mu = E / (2 * (1 + nu));
+        const double kappa = E / (3 * (1 - 2 * nu));
+        double D[9];
+        stiffness_inverse(lambda, mu, D);
+        o.lambda = (R)lambda;
+        o.mu = (R)mu;
+        o.kappa = (R)kappa;
+        for (int q = 0; q < 9; ++q) o.D[q] = (R)D[q];
+        o.yield_stress = (R)in.yield_stress;
+        o.hardening = (R)in.hardening;
+        o.hardening_law = in.hardening_law;
+        o.alpha_cap = (R)in.alpha_cap;
+        o.dlambda_cap = (R)in.dlambda_cap;
+        o.strain_cap = (R)in.strain_cap;
+        o.psi_cap = (R)in.psi_cap;
+        o.fracture_energy = (R)in.fracture_energy;
+        o.softening_onset = (R)in.softening_onset;
+        o.residual_fracture = (R)in.residual_fracture;
+        o.theta = (R)in.theta;
+        o.length_scale = (R)in.length_scale;
+        o.mobility = (R)in.mobility;
+    }
+    s.mobility = (R)d.materials[0].mobility;
+    s.wall_bc = d.wall_bc;
+    s.wall_layers = d.wall_layers;
+    fill_velocity_conditions<R>(d.slabs, d.n_slab_bcs, d.spheres, d.n_sphere_bcs, s.bc);
+    s.phase_field = d.phase_field;
+    s.fp64_svd_fallback = (d.precision == GMPM_PRECISION_FP32_FP64SVD);
+    s.svd_fallback_ratio = (R)d.svd_fallback_ratio;
+    s.dx_d = d.dx;
+    s.inv_dx_d = 1.0 / d.dx;
+}
+
+gmpm_status validate(const gmpm_scene_desc* d, const gmpm_particle_init* init) {
+    if (!d || !init || !init->positions || !init->masses) return GMPM_INVALID_ARG;
+    if (init->count <= 0 || init->count >= (int64_t(1) << 28)) return GMPM_INVALID_ARG;
+    if (!(d->dx > 0) || !(d->dt > 0) || !(d->particle_volume > 0)) return GMPM_INVALID_ARG;
+    for (int a = 0; a < 3; ++a)
+        if (d->grid_res[a] < 8 || d->grid_res[a] > 1019) return GMPM_INVALID_ARG;
+    if (d->n_materials < 1 || d->n_materials > GMPM_MAX_MATERIALS) return GMPM_INVALID_ARG;
+    for (int m = 0; m < d->n_materials; ++m) {
+        const gmpm_material& mt = d->materials[m];
+        if (!(mt.youngs_modulus > 0) || !(mt.poisson_ratio >= 0) || !(mt.poisson_ratio < 0.5)) return GMPM_INVALID_ARG;
+        if (!(mt.fracture_energy > 0)) return GMPM_INVALID_ARG;
+        if (mt.hardening_law != GMPM_HARDENING_EXPONENTIAL && mt.hardening_law != GMPM_HARDENING_LINEAR)
+            return GMPM_INVALID_ARG;
+    }
+    if (d->n_slab_bcs < 0 || d->n_slab_bcs > GMPM_MAX_SLAB_BCS) return GMPM_INVALID_ARG;
+    if (d->n_sphere_bcs < 0 || d->n_sphere_bcs > GMPM_MAX_SPHERE_BCS) return GMPM_INVALID_ARG;
+    for (int q = 0; q < d->n_slab_bcs; ++q)
+        if (d->slabs[q].axis < 0 || d->slabs[q].axis > 2) return GMPM_INVALID_ARG;
+    if (d->precision < 0 || d->precision > 2) return GMPM_INVALID_ARG;
+    if (d->phase_field < 0 || d->phase_field > 1) return GMPM_INVALID_ARG;
+    if (d->block_capacity < 0) return GMPM_INVALID_ARG;
+    if (init->material_ids)
+        for (int64_t p = 0; p < init->count; ++p)
+            if (init->material_ids[p] < 0 || init->material_ids[p] >= d->n_materials) return GMPM_INVALID_ARG;
+    return GMPM_OK;
+}
+
+int bit_width(unsigned v) {
+    int b = 0;
+    while (v) {
+        ++b;
+        v >>= 1;
+    }
+    return b;
+}
+
+inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+// Common scene interface, implemented per precision.
+struct SceneBase {
+    virtual ~SceneBase() {}
+    virtual gmpm_status substep(int n, cudaStream_t s) = 0;
+    virtual gmpm_status substep_timed(int n, cudaStream_t s, gmpm_stage_times* out) = 0;
+    virtual gmpm_status rebin(cudaStream_t s) = 0;
+    virtual gmpm_status read_particles(int field, int dtype, int order, void* dst, size_t bytes, cudaStream_t s) = 0;
+    virtual gmpm_status read_binning(int array, void* dst, size_t bytes) = 0;
+    virtual gmpm_status diagnostics(gmpm_diag* out) = 0;
+    virtual gmpm_status sync() = 0;
+    virtual gmpm_status set_velocity_conditions(const gmpm_slab_bc* slabs, int ns, const gmpm_sphere_bc* spheres,
+                                                int nsp, cudaStream_t s) = 0;
+};
+
+template <typename R>
+struct Scene : SceneBase {
+    gmpm_context* ctx = nullptr;
+    gmpm_scene_desc desc{};
+    int64_t n = 0;
+    int64_t stride = 0;  // plane stride (elements)
+    SceneDev<R>* d_sc = nullptr;
+    SceneDev<double>* d_sc64 = nullptr;
+    void* pstore = nullptr;
+    PState<R> st[2];
+    PAux<R> aux;
+    int cur = 0;
+    BinDev bin{};
+    ScanScratch scan{};
+    GridDev grid{};
+    Counters* d_cnt = nullptr;
+    double* d_pdiag = nullptr;  // [8]
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    std::vector<void*> allocs;
+    bool binned = false;  // binning of the current positions is valid
+    int64_t launches = 0;  // kernels launched by this scene
+    // kernels per launch_binning: keys, 3 scans x 3, mark, 2 compactions, links, hist, scatter, canon
+    static constexpr int kBinningKernels = 17;
+
+    ~Scene() override {
+        for (void* p : allocs) cudaFree(p);
+        if (staging) cudaFree(staging);
+        if (bc_staging) cudaFreeHost(bc_staging);
+        for (cudaEvent_t e : bc_done)
+            if (e) cudaEventDestroy(e);
+    }
+
+    template <typename T>
+    cudaError_t alloc(T** p, size_t count) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
+        if (e != cudaSuccess) return e;
+        allocs.push_back(q);
+        *p = reinterpret_cast<T*>(q);
+        return cudaSuccess;
+    }
+
+    LaunchCfg cfg() const { return LaunchCfg{ctx->num_sms, desc.deterministic}; }
+
+    gmpm_status create(gmpm_context* c, const gmpm_scene_desc* d, const gmpm_particle_init* init) {
+        ctx = c;
+        desc = *d;
+        n = init->count;
+        stride = (int64_t)round_up((size_t)n, 64);
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        // key space of the grid (page coordinates incl. the + neighbour page)
+        int maxb = 0;
+        for (int a = 0; a < 3; ++a) maxb = std::max(maxb, (d->grid_res[a] - 3) >> 2);
+        const int key_bits = bit_width((unsigned)(maxb + 1));
+        if (3 * key_bits + 6 > 32) return GMPM_INVALID_ARG;
+        const uint32_t key_space = 1u << (3 * key_bits);
+
+        SceneDev<R> h{};
+        fill_scene_dev<R>(desc, key_bits, h);
+        SceneDev<double> h64{};
+        fill_scene_dev<double>(desc, key_bits, h64);
+        GMPM_TRY(alloc(&d_sc, 1));
+        GMPM_TRY(alloc(&d_sc64, 1));
+        GMPM_TRY(cudaMemcpy(d_sc, &h, sizeof(h), cudaMemcpyHostToDevice));
+        GMPM_TRY(cudaMemcpy(d_sc64, &h64, sizeof(h64), cudaMemcpyHostToDevice));
+        GMPM_TRY(alloc(&d_cnt, 1));
+        GMPM_TRY(cudaMemset(d_cnt, 0, sizeof(Counters)));
+        GMPM_TRY(alloc(&d_pdiag, 8));
+        GMPM_TRY(alloc(&grid.diag, 8));
+        GMPM_TRY(cudaMemset(grid.diag, 0, 8 * sizeof(double)));
+
+        // particle planes: 2 x (x3 F9 c alpha psi m) + aux (v3 B9 sigma6 vol FP q3), + 2 id planes
+        const int state_planes = 16, aux_planes = 23;
+        const size_t nplanes = 2 * state_planes + aux_planes;
+        const size_t plane_bytes = round_up((size_t)stride * sizeof(R), 256);
+        const size_t id_bytes = round_up((size_t)stride * sizeof(uint32_t), 256);
+        GMPM_TRY(cudaMalloc(&pstore, nplanes * plane_bytes + 2 * id_bytes));
+        allocs.push_back(pstore);
+        char* base = reinterpret_cast<char*>(pstore);
+        auto next = [&]() {
+            R* p = reinterpret_cast<R*>(base);
+            base += plane_bytes;
+            return p;
+        };
+        for (int b = 0; b < 2; ++b) {
+            for (int a = 0; a < 3; ++a) st[b].x[a] = next();
+            for (int q = 0; q < 9; ++q) st[b].F[q] = next();
+            st[b].c = next();
+            st[b].alpha = next();
+            st[b].psi = next();
+            st[b].m = next();
+        }
+        for (int a = 0; a < 3; ++a) aux.v[a] = next();
+        for (int q = 0; q < 9; ++q) aux.B[q] = next();
+        for (int q = 0; q < 6; ++q) aux.sigma[q] = next();
+        aux.vol = next();
+        aux.FP = next();
+        for (int a = 0; a < 3; ++a) aux.q[a] = next();
+        for (int b = 0; b < 2; ++b) {
+            st[b].id = reinterpret_cast<uint32_t*>(base);
+            base += id_bytes;
+        }
+
+        // upload the initial state into buffer 0 (original order)
+        {
+            std::vector<R> tmp((size_t)n);
+            for (int a = 0; a < 3; ++a) {
+                for (int64_t p = 0; p < n; ++p) tmp[p] = (R)init->positions[3 * p + a];
+                GMPM_TRY(cudaMemcpy(st[0].x[a], tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
+                for (int64_t p = 0; p < n; ++p) tmp[p] = init->velocities ? (R)init->velocities[3 * p + a] : R(0);
+                GMPM_TRY(cudaMemcpy(aux.v[a], tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
+            }
+            for (int64_t p = 0; p < n; ++p) tmp[p] = (R)init->masses[p];
+            GMPM_TRY(cudaMemcpy(st[0].m, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
+            for (int q = 0; q < 9; ++q) {
+                const R v = (q % 4 == 0) ? R(1) : R(0);
+                for (int64_t p = 0; p < n; ++p) tmp[p] = v;
+                GMPM_TRY(cudaMemcpy(st[0].F[q], tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
+            }
+            for (int64_t p = 0; p < n; ++p) tmp[p] = R(1);
+            GMPM_TRY(cudaMemcpy(st[0].c, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
+            GMPM_TRY(cudaMemset(st[0].alpha, 0, n * sizeof(R)));
+            GMPM_TRY(cudaMemset(st[0].psi, 0, n * sizeof(R)));
+            std::vector<uint32_t> ids((size_t)n);
+            for (int64_t p = 0; p < n; ++p)
+                ids[p] = (uint32_t)p | ((uint32_t)(init->material_ids ? init->material_ids[p] : 0) << 28);
+            GMPM_TRY(cudaMemcpy(st[0].id, ids.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        }
+        GMPM_TRY(launch_init_stress<R>(d_sc, st[0], aux, n, d_cnt, 0));
+
+        // binning storage; page capacities from a first count on the device
+        bin.n = n;
+        bin.key_space = key_space;
+        GMPM_TRY(alloc(&bin.keys, (size_t)n));
+        GMPM_TRY(alloc(&bin.keys_sorted, (size_t)n));
+        GMPM_TRY(alloc(&bin.perm, (size_t)n));
+        GMPM_TRY(alloc(&bin.page_flag, key_space));
+        GMPM_TRY(alloc(&bin.page_rank, key_space));
+        GMPM_TRY(alloc(&bin.grid_flag, key_space));
+        GMPM_TRY(alloc(&bin.grid_rank, key_space));
+        int nb0 = 0, ng0 = 0;
+        {
+            // a provisional pass with tiny capacities only to count pages
+            bin.nb_cap = 1;
+            bin.ng_cap = 1;
+            const int64_t scan_n = key_space;
+            scan.capacity = scan_scratch_elems(scan_n);
+            int32_t* ts = nullptr;
+            GMPM_TRY(alloc(&ts, (size_t)scan.capacity));
+            scan.tile_sums = ts;
+            GMPM_TRY(count_pages(&nb0, &ng0));
+        }
+        int64_t nb_cap = desc.block_capacity > 0 ? desc.block_capacity : std::max<int64_t>(2 * (int64_t)nb0, nb0 + 256);
+        int64_t ng_cap = std::max<int64_t>(2 * (int64_t)ng0, ng0 + 512);
+        if (desc.block_capacity > 0) ng_cap = std::max<int64_t>(ng_cap, std::min<int64_t>(8 * nb_cap, key_space));
+        nb_cap = std::min<int64_t>(nb_cap, key_space);
+        ng_cap = std::min<int64_t>(ng_cap, key_space);
+        if (nb_cap < nb0) return GMPM_TABLE_OVERFLOW;
+        bin.nb_cap = (int32_t)nb_cap;
+        bin.ng_cap = (int32_t)ng_cap;
+        GMPM_TRY(alloc(&bin.block_keys, (size_t)nb_cap));
+        GMPM_TRY(alloc(&bin.cell_count, (size_t)nb_cap * 64));
+        GMPM_TRY(alloc(&bin.cell_start, (size_t)nb_cap * 64 + 1));
+        GMPM_TRY(alloc(&bin.grid_keys, (size_t)ng_cap));
+        GMPM_TRY(alloc(&bin.adj, (size_t)nb_cap * 8));
+        GMPM_TRY(alloc(&bin.grid_src, (size_t)ng_cap * 8));
+        {
+            const int64_t scan_n = std::max<int64_t>(key_space, nb_cap * 64);
+            scan.capacity = scan_scratch_elems(scan_n);
+            int32_t* ts = nullptr;
+            GMPM_TRY(alloc(&ts, (size_t)scan.capacity));
+            scan.tile_sums = ts;
+        }
+        R* tile = nullptr;
+        R* nodes = nullptr;
+        GMPM_TRY(alloc(&tile, (size_t)nb_cap * kP2GChannels * kWindowNodes));
+        GMPM_TRY(alloc(&nodes, (size_t)ng_cap * kGridChannels * 64));
+        grid.tile = tile;
+        grid.nodes = nodes;
+        GMPM_TRY(prepare_p2g<R>());
+        GMPM_TRY(prepare_g2p<R>());
+        GMPM_TRY(cudaMemset(d_cnt, 0, sizeof(Counters)));
+        GMPM_TRY(cudaDeviceSynchronize());
+        return GMPM_OK;
+    }
+
+    // Count active and grid pages of the current positions (creation only).
+    cudaError_t count_pages(int* nb, int* ng) {
+        const int T = 256;
+        const unsigned gk = (bin.key_space + T - 1) / T;
+        cudaMemset(bin.page_flag, 0, bin.key_space);
+        cudaMemset(bin.grid_flag, 0, bin.key_space);
+        launch_keys_only(0);
+        scan_exclusive<uint8_t>(bin.page_flag, bin.page_rank, (int64_t)bin.key_space, &d_cnt->n_blocks, scan, 0);
+        mark_grid(0);
+        scan_exclusive<uint8_t>(bin.grid_flag, bin.grid_rank, (int64_t)bin.key_space, &d_cnt->n_grid_blocks, scan, 0);
+        (void)gk;
+        Counters h{};
+        cudaError_t e = cudaMemcpy(&h, d_cnt, sizeof(h), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return e;
+        *nb = h.n_blocks;
+        *ng = h.n_grid_blocks;
+        return cudaGetLastError();
+    }
+    void launch_keys_only(cudaStream_t s);
+    void mark_grid(cudaStream_t s);
+
+    gmpm_status do_bin(cudaStream_t s) {
+        GMPM_TRY(launch_binning<R>(d_sc, st[cur], bin, scan, d_cnt, ctx->num_sms, s));
+        binned = true;
+        return GMPM_OK;
+    }
+
+    // One substep; ev (optional) receives events after bin, p2g, grid, g2p.
+    gmpm_status one_substep(cudaStream_t s, cudaEvent_t* ev) {
+        gmpm_status r = do_bin(s);
+        if (r != GMPM_OK) return r;
+        launches += kBinningKernels;
+        if (ev) GMPM_TRY(cudaEventRecord(ev[0], s));
+        GMPM_TRY(launch_p2g<R>(d_sc, st[cur], aux, bin, grid, d_cnt, cfg(), s));
+        if (ev) GMPM_TRY(cudaEventRecord(ev[1], s));
+        GMPM_TRY(launch_grid<R>(d_sc, bin, grid, d_cnt, cfg(), s));
+        if (ev) GMPM_TRY(cudaEventRecord(ev[2], s));
+        GMPM_TRY(launch_g2p<R>(d_sc, desc.precision == GMPM_PRECISION_FP32_FP64SVD ? d_sc64 : nullptr, st[cur],
+                               st[1 - cur], aux, bin, grid, d_cnt, cfg(), s, desc.dt));
+        if (ev) GMPM_TRY(cudaEventRecord(ev[3], s));
+        launches += 4;  // p2g, grid, g2p, clock advance
+        cur = 1 - cur;
+        binned = false;
+        return GMPM_OK;
+    }
+
+    gmpm_status substep(int nsteps, cudaStream_t s) override {
+        if (nsteps < 0) return GMPM_INVALID_ARG;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        for (int it = 0; it < nsteps; ++it) {
+            gmpm_status r = one_substep(s, nullptr);
+            if (r != GMPM_OK) return r;
+        }
+        return GMPM_OK;
+    }
+
+    gmpm_status substep_timed(int nsteps, cudaStream_t s, gmpm_stage_times* out) override {
+        if (nsteps < 0 || !out) return GMPM_INVALID_ARG;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        std::memset(out, 0, sizeof(*out));
+        std::vector<cudaEvent_t> ev((size_t)nsteps * 5);
+        for (auto& e : ev) GMPM_TRY(cudaEventCreate(&e));
+        gmpm_status r = GMPM_OK;
+        for (int it = 0; it < nsteps && r == GMPM_OK; ++it) {
+            cudaEvent_t* e = &ev[(size_t)it * 5];
+            cudaEventRecord(e[0], s);
+            r = one_substep(s, e + 1);
+        }
+        cudaError_t ce = cudaEventSynchronize(ev.back());
+        if (r == GMPM_OK && ce == cudaSuccess) {
+            for (int it = 0; it < nsteps; ++it) {
+                cudaEvent_t* e = &ev[(size_t)it * 5];
+                float t[4];
+                for (int q = 0; q < 4; ++q) cudaEventElapsedTime(&t[q], e[q], e[q + 1]);
+                out->bin_ms += t[0];
+                out->p2g_ms += t[1];
+                out->grid_ms += t[2];
+                out->g2p_ms += t[3];
+                out->total_ms += t[0] + t[1] + t[2] + t[3];
+            }
+            out->substeps = nsteps;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        if (r != GMPM_OK) return r;
+        return cuda_status(ce);
+    }
+
+    gmpm_status rebin(cudaStream_t s) override {
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        launches += kBinningKernels;
+        return do_bin(s);
+    }
+
+    gmpm_status read_particles(int field, int dtype, int order, void* dst, size_t bytes, cudaStream_t s) override {
+        const int nc = field_components(field);
+        if (nc == 0 || !dst) return GMPM_INVALID_ARG;
+        if (dtype < 0 || dtype > 2 || order < 0 || order > 1) return GMPM_INVALID_ARG;
+        const size_t esz = dtype == GMPM_DTYPE_F64 ? 8 : 4;
+        const size_t need = (size_t)n * nc * esz;
+        if (bytes < need) return GMPM_INVALID_ARG;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        cudaPointerAttributes attr{};
+        bool on_device = false;
+        if (cudaPointerGetAttributes(&attr, dst) == cudaSuccess)
+            on_device = (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged);
+        else
+            cudaGetLastError();
+        if (on_device) {
+            GMPM_TRY(launch_pack_field<R>(st[cur], aux, field, dtype, order, n, dst, s));
+            GMPM_TRY(cudaStreamSynchronize(s));
+            return GMPM_OK;
+        }
+        if (staging_bytes < need) {
+            if (staging) cudaFree(staging);
+            staging = nullptr;
+            staging_bytes = 0;
+            GMPM_TRY(cudaMalloc(&staging, need));
+            staging_bytes = need;
+        }
+        GMPM_TRY(launch_pack_field<R>(st[cur], aux, field, dtype, order, n, staging, s));
+        GMPM_TRY(cudaMemcpyAsync(dst, staging, need, cudaMemcpyDefault, s));
+        GMPM_TRY(cudaStreamSynchronize(s));
+        return GMPM_OK;
+    }
+
+    gmpm_status read_binning(int array, void* dst, size_t bytes) override {
+        if (!dst) return GMPM_INVALID_ARG;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        GMPM_TRY(cudaDeviceSynchronize());
+        Counters h{};
+        GMPM_TRY(cudaMemcpy(&h, d_cnt, sizeof(h), cudaMemcpyDeviceToHost));
+        const int64_t nb = std::min(h.n_blocks, bin.nb_cap), ng = std::min(h.n_grid_blocks, bin.ng_cap);
+        auto copy = [&](const void* src, size_t sz) -> gmpm_status {
+            if (bytes < sz) return GMPM_INVALID_ARG;
+            GMPM_TRY(cudaMemcpy(dst, src, sz, cudaMemcpyDeviceToHost));
+            return GMPM_OK;
+        };
+        switch (array) {
+            case GMPM_BIN_COUNTS: {
+                if (bytes < 4 * sizeof(int64_t)) return GMPM_INVALID_ARG;
+                int64_t* o = reinterpret_cast<int64_t*>(dst);
+                o[0] = n;
+                o[1] = h.n_blocks;
+                o[2] = h.n_grid_blocks;
+                o[3] = bin.key_space;
+                return GMPM_OK;
+            }
+            case GMPM_BIN_PERM: return copy(bin.perm, n * 4);
+            case GMPM_BIN_KEYS: return copy(bin.keys_sorted, n * 4);
+            case GMPM_BIN_BLOCK_KEYS: return copy(bin.block_keys, nb * 4);
+            case GMPM_BIN_BLOCK_START: {
+                if (bytes < (size_t)(nb + 1) * 4) return GMPM_INVALID_ARG;
+                std::vector<int32_t> cs((size_t)nb * 64 + 1);
+                GMPM_TRY(cudaMemcpy(cs.data(), bin.cell_start, cs.size() * 4, cudaMemcpyDeviceToHost));
+                int32_t* o = reinterpret_cast<int32_t*>(dst);
+                for (int64_t b = 0; b <= nb; ++b) o[b] = cs[b * 64];
+                return GMPM_OK;
+            }
+            case GMPM_BIN_CELL_START: return copy(bin.cell_start, (nb * 64 + 1) * 4);
+            case GMPM_BIN_GRID_KEYS: return copy(bin.grid_keys, ng * 4);
+            case GMPM_BIN_ADJ: return copy(bin.adj, nb * 8 * 4);
+            default: return GMPM_INVALID_ARG;
+        }
+    }
+
+    gmpm_status diagnostics(gmpm_diag* out) override {
+        if (!out) return GMPM_INVALID_ARG;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        GMPM_TRY(launch_particle_diag<R>(st[cur], aux, n, d_pdiag, 0));
+        GMPM_TRY(cudaDeviceSynchronize());
+        double pd[8], gd[8];
+        Counters h{};
+        GMPM_TRY(cudaMemcpy(pd, d_pdiag, sizeof(pd), cudaMemcpyDeviceToHost));
+        GMPM_TRY(cudaMemcpy(gd, grid.diag, sizeof(gd), cudaMemcpyDeviceToHost));
+        GMPM_TRY(cudaMemcpy(&h, d_cnt, sizeof(h), cudaMemcpyDeviceToHost));
+        std::memset(out, 0, sizeof(*out));
+        out->particle_mass = pd[0];
+        for (int a = 0; a < 3; ++a) {
+            out->particle_momentum[a] = pd[1 + a];
+            out->grid_momentum[a] = gd[1 + a];
+        }
+        out->grid_mass = gd[0];
+        out->kinetic_energy = pd[4];
+        out->max_speed = pd[5];
+        out->min_damage = pd[6];
+        out->time = h.time;
+        out->substeps = h.substeps;
+        out->n_particles = n;
+        out->n_blocks = h.n_blocks;
+        out->n_grid_blocks = h.n_grid_blocks;
+        out->flags = h.flags;
+        out->kernel_launches = launches;
+        return GMPM_OK;
+    }
+
+    // Two pinned host staging blocks for velocity-condition updates, so an
+    // update can be written while the previous copy is still in flight.
+    VelocityConditions<R>* bc_staging = nullptr;  // [2]
+    cudaEvent_t bc_done[2] = {nullptr, nullptr};
+    int bc_next = 0;
+
+    gmpm_status set_velocity_conditions(const gmpm_slab_bc* slabs, int ns, const gmpm_sphere_bc* spheres, int nsp,
+                                        cudaStream_t s) override {
+        if (ns < 0 || ns > GMPM_MAX_SLAB_BCS || nsp < 0 || nsp > GMPM_MAX_SPHERE_BCS) return GMPM_INVALID_ARG;
+        if ((ns > 0 && !slabs) || (nsp > 0 && !spheres)) return GMPM_INVALID_ARG;
+        for (int q = 0; q < ns; ++q)
+            if (slabs[q].axis < 0 || slabs[q].axis > 2) return GMPM_INVALID_ARG;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        if (!bc_staging) {
+            GMPM_TRY(cudaMallocHost(reinterpret_cast<void**>(&bc_staging), 2 * sizeof(*bc_staging)));
+            GMPM_TRY(cudaEventCreateWithFlags(&bc_done[0], cudaEventDisableTiming));
+            GMPM_TRY(cudaEventCreateWithFlags(&bc_done[1], cudaEventDisableTiming));
+            GMPM_TRY(cudaEventRecord(bc_done[0], s));
+            GMPM_TRY(cudaEventRecord(bc_done[1], s));
+        }
+        const int k = bc_next;
+        bc_next ^= 1;
+        GMPM_TRY(cudaEventSynchronize(bc_done[k]));  // the copy that last read block k has left
+        fill_velocity_conditions<R>(slabs, ns, spheres, nsp, bc_staging[k]);
+        GMPM_TRY(cudaMemcpyAsync(&d_sc->bc, &bc_staging[k], sizeof(VelocityConditions<R>), cudaMemcpyHostToDevice, s));
+        GMPM_TRY(cudaEventRecord(bc_done[k], s));
+        desc.n_slab_bcs = ns;
+        desc.n_sphere_bcs = nsp;
+        for (int q = 0; q < ns; ++q) desc.slabs[q] = slabs[q];
+        for (int q = 0; q < nsp; ++q) desc.spheres[q] = spheres[q];
+        return GMPM_OK;
+    }
+
+    gmpm_status sync() override {
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        GMPM_TRY(cudaDeviceSynchronize());
+        Counters h{};
+        GMPM_TRY(cudaMemcpy(&h, d_cnt, sizeof(h), cudaMemcpyDeviceToHost));
+        if (h.flags & GMPM_FLAG_TABLE_OVERFLOW) return GMPM_TABLE_OVERFLOW;
+        if (h.flags & GMPM_FLAG_OUT_OF_DOMAIN) return GMPM_OUT_OF_DOMAIN;
+        if (h.flags & GMPM_FLAG_NONFINITE) return GMPM_NONFINITE;
+        return GMPM_OK;
+    }
+};
+
+}  // namespace gmpm
+
+// ---- key-only helpers used at creation (declared in Scene) ----------------
+namespace gmpm {
+template <typename R>
+void Scene<R>::launch_keys_only(cudaStream_t s) {
+    launch_keys<R>(d_sc, st[cur], bin, d_cnt, s);
+}
+template <typename R>
+void Scene<R>::mark_grid(cudaStream_t s) {
+    launch_mark_grid(bin, s);
+}
+}  // namespace gmpm
+
+struct gmpm_scene {
+    gmpm::SceneBase* impl;
+};
+
+extern "C" {
+
+const char* gmpm_status_string(gmpm_status s) {
+    switch (s) {
+        case GMPM_OK: return "ok";
+        case GMPM_INVALID_ARG: return "invalid argument";
+        case GMPM_OOM: return "out of device memory";
+        case GMPM_TABLE_OVERFLOW: return "page table capacity exceeded";
+        case GMPM_NONFINITE: return "non-finite particle state";
+        case GMPM_OUT_OF_DOMAIN: return "particle stencil outside the grid";
+        case GMPM_CUDA_ERROR: return "CUDA error";
+        case GMPM_NOT_SUPPORTED: return "not supported";
+        case GMPM_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+gmpm_status gmpm_context_create(int device, gmpm_context** out) {
+    if (!out) return GMPM_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return GMPM_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return GMPM_INVALID_ARG;
+    gmpm_context* c = new (std::nothrow) gmpm_context();
+    if (!c) return GMPM_OOM;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaGetDeviceProperties(&c->prop, device) != cudaSuccess) {
+        delete c;
+        return GMPM_CUDA_ERROR;
+    }
+    c->num_sms = c->prop.multiProcessorCount;
+    *out = c;
+    return GMPM_OK;
+}
+
+gmpm_status gmpm_context_destroy(gmpm_context* ctx) {
+    if (!ctx) return GMPM_INVALID_ARG;
+    delete ctx;
+    return GMPM_OK;
+}
+
+gmpm_status gmpm_scene_desc_reference_defaults(gmpm_scene_desc* d, double dx, int rx, int ry, int rz) {
+    if (!d || !(dx > 0)) return GMPM_INVALID_ARG;
+    std::memset(d, 0, sizeof(*d));
+    d->dx = dx;
+    d->grid_res[0] = rx;
+    d->grid_res[1] = ry;
+    d->grid_res[2] = rz;
+    d->dt = 1e-4;                                  // Simulator.cpp:172
+    d->gravity[1] = -10.0;                         // TimeIntegrator.cu:100
+    d->particle_volume = dx * dx * dx / 8.0;
+    d->n_materials = 1;
+    gmpm_material& m = d->materials[0];
+    m.youngs_modulus = 2e2;                        // Simulator.cpp:114-116 (scene 1)
+    m.poisson_ratio = 0.4;
+    m.density = 3.0;
+    m.yield_stress = 800.0;                        // ExplicitTimeIntegrator.cu:188
+    m.hardening_law = GMPM_HARDENING_EXPONENTIAL;
+    m.hardening = 3.0;                             // :189
+    m.alpha_cap = 1.0;                             // :194
+    m.dlambda_cap = 100.0;                         // :217-220
+    m.strain_cap = 3.0;                            // :267-271
+    m.psi_cap = 1e6;                               // :313
+    m.fracture_energy = 3.0;                       // :317
+    m.softening_onset = 0.01;                      // :320
+    m.residual_fracture = 0.1;                     // :327
+    m.theta = (double)0.0001f;                     // :334 (float)
+    m.length_scale = 0.5 * dx;                     // :335
+    m.mobility = 50.0;                             // Materials.cpp:13
+    d->wall_bc = 1;
+    d->wall_layers = 4;
+    d->precision = GMPM_PRECISION_FP32;
+    d->phase_field = GMPM_PHASE_FIELD_EXPLICIT;
+    d->deterministic = 1;
+    d->svd_fallback_ratio = 1e-3;
+    return GMPM_OK;
+}
+
+gmpm_status gmpm_scene_create(gmpm_context* ctx, const gmpm_scene_desc* desc, const gmpm_particle_init* init,
+                              gmpm_scene** out) {
+    if (!ctx || !out) return GMPM_INVALID_ARG;
+    *out = nullptr;
+    gmpm_status v = gmpm::validate(desc, init);
+    if (v != GMPM_OK) return v;
+    gmpm_scene* s = new (std::nothrow) gmpm_scene();
+    if (!s) return GMPM_OOM;
+    gmpm_status r;
+    if (desc->precision == GMPM_PRECISION_FP64) {
+        auto* impl = new (std::nothrow) gmpm::Scene<double>();
+        s->impl = impl;
+        r = impl ? impl->create(ctx, desc, init) : GMPM_OOM;
+    } else {
+        auto* impl = new (std::nothrow) gmpm::Scene<float>();
+        s->impl = impl;
+        r = impl ? impl->create(ctx, desc, init) : GMPM_OOM;
+    }
+    if (r != GMPM_OK) {
+        delete s->impl;
+        delete s;
+        cudaGetLastError();
+        return r;
+    }
+    *out = s;
+    return GMPM_OK;
+}
+
+gmpm_status gmpm_scene_destroy(gmpm_scene* s) {
+    if (!s) return GMPM_INVALID_ARG;
+    delete s->impl;
+    delete s;
+    return GMPM_OK;
+}
+
+gmpm_status gmpm_substep(gmpm_scene* s, int n, void* stream) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->substep(n, reinterpret_cast<cudaStream_t>(stream));
+}
+
+gmpm_status gmpm_substep_timed(gmpm_scene* s, int n, void* stream, gmpm_stage_times* out) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->substep_timed(n, reinterpret_cast<cudaStream_t>(stream), out);
+}
+
+gmpm_status gmpm_rebin(gmpm_scene* s, void* stream) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->rebin(reinterpret_cast<cudaStream_t>(stream));
+}
+
+gmpm_status gmpm_scene_sync(gmpm_scene* s) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->sync();
+}
+
+gmpm_status gmpm_read_particles(gmpm_scene* s, int field, int dtype, int order, void* dst, size_t bytes,
+                                void* stream) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->read_particles(field, dtype, order, dst, bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+gmpm_status gmpm_set_velocity_conditions(gmpm_scene* s, const gmpm_slab_bc* slabs, int n_slabs,
+                                         const gmpm_sphere_bc* spheres, int n_spheres, void* stream) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->set_velocity_conditions(slabs, n_slabs, spheres, n_spheres, reinterpret_cast<cudaStream_t>(stream));
+}
+
+gmpm_status gmpm_read_binning(gmpm_scene* s, int array, void* dst, size_t bytes) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->read_binning(array, dst, bytes);
+}
+
+gmpm_status gmpm_diagnostics(gmpm_scene* s, gmpm_diag* out) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->diagnostics(out);
+}
+
+}  // extern "C"

@@ -1,0 +1,249 @@
+// Particle binning by SPGrid page/cell key, replacing the reference's hash +
+// counting sort (Particles::sort_by_offsets, Particle_kernal.cu:158-249,484-542)
+// and DomainTransformer::rebuild (Transformer_kernal.cu:15-209).
+//
+// Instead of an open-addressing page hash with unbounded probes and host
+// syncs, pages are marked in a dense page-key table (the key space of the
+// scene's grid), ranked by an exclusive scan (ascending page key = canonical
+// page ids), and the +x/+y/+z neighbour pages are found by the same table.
+// Particles are counting-sorted by (page rank, cell); the in-cell order is
+// then made canonical (ascending previous slot), so the result equals a
+// stable sort by (key, previous slot) bit for bit.  No host synchronisation.
+#include <cstdint>
+
+#include "kernels.h"
+#include "scan.cuh"
+
+namespace gmpm {
+
+template <typename R>
+__global__ void k_bin_keys(int64_t n, const R* __restrict__ x0, const R* __restrict__ x1, const R* __restrict__ x2,
+                           const SceneDev<R>* __restrict__ sc, uint32_t* __restrict__ keys,
+                           uint8_t* __restrict__ page_flag, Counters* cnt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double inv_dx = sc->inv_dx_d;
+    const double xs[3] = {(double)x0[i], (double)x1[i], (double)x2[i]};
+    int base[3];
+    bool bad = false;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        // (int)(x / dx + 0.5) - 1 as in cal_cellId (Particle_kernal.cu:162-164),
+        // valid when the 3-node stencil stays inside the grid.
+        const double t = __dadd_rn(__dmul_rn(xs[a], inv_dx), 0.5);
+        const int hi = sc->res[a] - 3;
+        if (!(t >= 1.0)) {
+            base[a] = 0;
+            bad = true;
+        } else if (t >= (double)(hi + 2)) {
+            base[a] = hi;
+            bad = true;
+        } else {
+            base[a] = (int)t - 1;
+        }
+    }
+    if (bad) raise_flag(cnt, GMPM_FLAG_OUT_OF_DOMAIN);
+    const uint32_t cell = (uint32_t)(((base[0] & 3) << 4) | ((base[1] & 3) << 2) | (base[2] & 3));
+    const uint32_t pk = page_key(base[0] >> 2, base[1] >> 2, base[2] >> 2);
+    keys[i] = (pk << 6) | cell;
+    page_flag[pk] = 1;
+}
+
+// Mark every active page and its 7 "+" neighbours as grid pages
+// (supplementAdjacentPages, Transformer_kernal.cu:70-96).
+__global__ void k_mark_grid(uint32_t key_space, const uint8_t* __restrict__ page_flag, uint8_t* __restrict__ grid_flag) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= key_space || !page_flag[k]) return;
+    int bx, by, bz;
+    page_coords(k, bx, by, bz);
+#pragma unroll
+    for (int d = 0; d < 8; ++d) grid_flag[page_key(bx + (d >> 2), by + ((d >> 1) & 1), bz + (d & 1))] = 1;
+}
+
+// Compact flagged keys into ascending order.
+__global__ void k_compact_keys(uint32_t key_space, const uint8_t* __restrict__ flag, const int32_t* __restrict__ rank,
+                               uint32_t* __restrict__ out, int cap, Counters* cnt) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= key_space || !flag[k]) return;
+    const int r = rank[k];
+    if (r < cap)
+        out[r] = k;
+    else
+        raise_flag(cnt, GMPM_FLAG_TABLE_OVERFLOW);
+}
+
+// Page topology: adj (establishPageTopology, Transformer_kernal.cu:98-114) and
+// its inverse grid_src used by the fixed-order grid gather.
+__global__ void k_page_links(BinDev bin, const Counters* cnt) {
+    const int nb = min(cnt->n_blocks, bin.nb_cap);
+    const int ng = min(cnt->n_grid_blocks, bin.ng_cap);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = t & 7;
+    const int idx = t >> 3;
+    const int di = slot >> 2, dj = (slot >> 1) & 1, dk = slot & 1;
+    if (idx < nb) {
+        int bx, by, bz;
+        page_coords(bin.block_keys[idx], bx, by, bz);
+        const int r = bin.grid_rank[page_key(bx + di, by + dj, bz + dk)];
+        bin.adj[idx * 8 + slot] = (r < bin.ng_cap) ? r : -1;  // overflow is flagged by k_compact_keys
+    }
+    if (idx < ng) {
+        int gx, gy, gz;
+        page_coords(bin.grid_keys[idx], gx, gy, gz);
+        int src = -1;
+        if (gx - di >= 0 && gy - dj >= 0 && gz - dk >= 0) {
+            const uint32_t k = page_key(gx - di, gy - dj, gz - dk);
+            if (k < bin.key_space && bin.page_flag[k]) {
+                const int r = bin.page_rank[k];
+                src = (r < bin.nb_cap) ? r : -1;
+            }
+        }
+        bin.grid_src[idx * 8 + slot] = src;
+    }
+}
+
+// Histogram of (page rank, cell) buckets with warp-aggregated atomics.
+__global__ void k_bin_hist(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
+                           int32_t* __restrict__ cell_count, int nb_cap) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    int bucket = -1;
+    if (live) {
+        const uint32_t key = keys[i];
+        const int r = page_rank[key >> 6];
+        if (r < nb_cap) bucket = r * 64 + (int)(key & 63);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, bucket);
+    const int lane = threadIdx.x & 31;
+    if (bucket >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cell_count[bucket], __popc(peers));
+}
+
+// Scatter slots; lanes of one warp with the same bucket keep their order.
+__global__ void k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
+                              const int32_t* __restrict__ cell_start, int32_t* __restrict__ fill,
+                              int32_t* __restrict__ perm, uint32_t* __restrict__ keys_sorted, int nb_cap) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    int bucket = -1;
+    uint32_t key = 0;
+    if (live) {
+        key = keys[i];
+        const int r = page_rank[key >> 6];
+        if (r < nb_cap) bucket = r * 64 + (int)(key & 63);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, bucket);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (bucket >= 0 && lane == leader) base = atomicAdd(&fill[bucket], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (bucket < 0) return;
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    const int slot = cell_start[bucket] + base + rank;
+    perm[slot] = (int32_t)i;
+    keys_sorted[slot] = key;
+}
+
+// Canonical in-cell order: ascending previous slot.  One CTA per page; the
+// page's slots are ranked in shared memory (cells hold few particles).
+constexpr int kCanonBuf = 4096;
+__global__ void __launch_bounds__(256) k_bin_canon(BinDev bin, const Counters* cnt) {
+    __shared__ int32_t buf[kCanonBuf];
+    const int nb = min(cnt->n_blocks, bin.nb_cap);
+    for (int b = blockIdx.x; b < nb; b += gridDim.x) {
+        const int32_t* cs = bin.cell_start + (int64_t)b * 64;
+        const int bs = cs[0], be = cs[64];
+        // Process whole cells in windows that fit the buffer.
+        int c0 = 0;
+        while (c0 < 64) {
+            int c1 = c0;
+            while (c1 < 64 && cs[c1 + 1] - cs[c0] <= kCanonBuf) ++c1;
+            if (c1 == c0) {
+                // A single cell larger than the buffer: rank directly in global
+                // memory using `keys` (free after the scatter) as staging.
+                const int lo = cs[c0], hi = cs[c0 + 1];
+                for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+                    const int32_t v = bin.perm[s];
+                    int r = 0;
+                    for (int u = lo; u < hi; ++u) r += bin.perm[u] < v;
+                    bin.keys[lo + r] = (uint32_t)v;
+                }
+                __syncthreads();
+                for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) bin.perm[s] = (int32_t)bin.keys[s];
+                __syncthreads();
+                c0 = c0 + 1;
+                continue;
+            }
+            const int lo = cs[c0], hi = cs[c1];
+            for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) buf[s - lo] = bin.perm[s];
+            __syncthreads();
+            for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+                const int cell = (int)(bin.keys_sorted[s] & 63);
+                const int a = cs[cell] - lo, e = cs[cell + 1] - lo;
+                const int32_t v = buf[s - lo];
+                int r = 0;
+                for (int u = a; u < e; ++u) r += buf[u] < v;
+                bin.perm[lo + a + r] = v;
+            }
+            __syncthreads();
+            c0 = c1;
+        }
+        (void)bs;
+        (void)be;
+    }
+}
+
+// ---------------------------------------------------------------------------
+
+template <typename R>
+cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bin, ScanScratch scan, Counters* cnt,
+                           int num_sms, cudaStream_t stream) {
+    const int64_t n = bin.n;
+    const int T = 256;
+    const unsigned gn = (unsigned)((n + T - 1) / T);
+    const unsigned gk = (bin.key_space + T - 1) / T;
+    cudaMemsetAsync(bin.page_flag, 0, bin.key_space, stream);
+    cudaMemsetAsync(bin.grid_flag, 0, bin.key_space, stream);
+    k_bin_keys<R><<<gn, T, 0, stream>>>(n, st.x[0], st.x[1], st.x[2], sc, bin.keys, bin.page_flag, cnt);
+    scan_exclusive<uint8_t>(bin.page_flag, bin.page_rank, (int64_t)bin.key_space, &cnt->n_blocks, scan, stream);
+    k_mark_grid<<<gk, T, 0, stream>>>(bin.key_space, bin.page_flag, bin.grid_flag);
+    scan_exclusive<uint8_t>(bin.grid_flag, bin.grid_rank, (int64_t)bin.key_space, &cnt->n_grid_blocks, scan, stream);
+    k_compact_keys<<<gk, T, 0, stream>>>(bin.key_space, bin.page_flag, bin.page_rank, bin.block_keys, bin.nb_cap, cnt);
+    k_compact_keys<<<gk, T, 0, stream>>>(bin.key_space, bin.grid_flag, bin.grid_rank, bin.grid_keys, bin.ng_cap, cnt);
+    const int links = max(bin.nb_cap, bin.ng_cap) * 8;
+    k_page_links<<<(links + T - 1) / T, T, 0, stream>>>(bin, cnt);
+    const int64_t ncell = (int64_t)bin.nb_cap * 64;
+    cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), stream);
+    k_bin_hist<<<gn, T, 0, stream>>>(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap);
+    scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, ncell, bin.cell_start + ncell, scan, stream);
+    cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), stream);
+    k_bin_scatter<<<gn, T, 0, stream>>>(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, bin.perm,
+                                        bin.keys_sorted, bin.nb_cap);
+    k_bin_canon<<<num_sms * 4, 256, 0, stream>>>(bin, cnt);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_keys(const SceneDev<R>* sc, const PState<R>& st, BinDev bin, Counters* cnt, cudaStream_t s) {
+    const int T = 256;
+    k_bin_keys<R><<<(unsigned)((bin.n + T - 1) / T), T, 0, s>>>(bin.n, st.x[0], st.x[1], st.x[2], sc, bin.keys,
+                                                                 bin.page_flag, cnt);
+    return cudaGetLastError();
+}
+template cudaError_t launch_keys<float>(const SceneDev<float>*, const PState<float>&, BinDev, Counters*,
+                                        cudaStream_t);
+template cudaError_t launch_keys<double>(const SceneDev<double>*, const PState<double>&, BinDev, Counters*,
+                                         cudaStream_t);
+
+cudaError_t launch_mark_grid(BinDev bin, cudaStream_t s) {
+    const int T = 256;
+    k_mark_grid<<<(bin.key_space + T - 1) / T, T, 0, s>>>(bin.key_space, bin.page_flag, bin.grid_flag);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_binning<float>(const SceneDev<float>*, const PState<float>&, BinDev, ScanScratch,
+                                           Counters*, int, cudaStream_t);
+template cudaError_t launch_binning<double>(const SceneDev<double>*, const PState<double>&, BinDev, ScanScratch,
+                                            Counters*, int, cudaStream_t);
+
+}  // namespace gmpm

@@ -1,0 +1,116 @@
+// Shared device definitions: scene parameters as the kernels see them, SPGrid
+// page keys, status flags.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gmpm.h"
+
+namespace gmpm {
+
+constexpr int kMaxMaterials = GMPM_MAX_MATERIALS;
+constexpr int kCellsPerBlock = 64;   // 4x4x4 nodes per SPGrid page (SPGridMask.cpp:76-89)
+constexpr int kWindow = 6;           // a page's particles touch a 6x6x6 node window
+constexpr int kWindowNodes = 216;
+
+// P2G channels written to the per-page tile scratch.  Momentum already
+// includes dt * force (the reference adds f*dt/m after dividing p by m,
+// TimeIntegrator.cu:96-107; both are sums over the same particles).
+enum P2GChannel : int {
+    CH_M = 0,      // sum m w
+    CH_P0 = 1,     // sum m w (v + B D^-1 (x_i - x_p)) - dt V0 P F^T grad w
+    CH_P1 = 2,
+    CH_P2 = 3,
+    CH_CW = 4,     // sum w c
+    CH_W = 5,      // sum w
+    CH_VW = 6,     // sum V w
+    CH_VWFP = 7,   // sum V w FP
+    CH_KC = 8,     // sum grad w . (4 L0^2 V grad c)
+    kP2GChannels = 9
+};
+
+// Grid channels read by G2P.
+enum GridChannel : int { GC_V0 = 0, GC_V1 = 1, GC_V2 = 2, GC_DC = 3, GC_CN = 4, kGridChannels = 5 };
+
+// Per-material constants in the precision of the kernel.
+template <typename Real>
+struct MaterialDev {
+    Real lambda, mu, kappa;
+    Real D[9];              // inverse of the isotropic stiffness (Gauss-Jordan as in Inverse())
+    Real yield_stress, hardening;
+    int hardening_law;
+    Real alpha_cap, dlambda_cap, strain_cap, psi_cap;
+    Real fracture_energy, softening_onset, residual_fracture;
+    Real theta, length_scale, mobility;
+};
+
+// Velocity conditions: axis-aligned slabs and moving spheres.  Kept as one
+// contiguous block so the host can replace it with a single copy.
+template <typename Real>
+struct VelocityConditions {
+    int n_slabs, n_spheres;
+    int slab_axis[GMPM_MAX_SLAB_BCS];
+    Real slab_lo[GMPM_MAX_SLAB_BCS], slab_hi[GMPM_MAX_SLAB_BCS], slab_vel[GMPM_MAX_SLAB_BCS][3];
+    Real sph_c[GMPM_MAX_SPHERE_BCS][3], sph_r[GMPM_MAX_SPHERE_BCS], sph_v[GMPM_MAX_SPHERE_BCS][3];
+};
+
+template <typename Real>
+struct SceneDev {
+    Real dx, inv_dx, dt;
+    Real Dinv;              // 4 / dx^2 (Setting.h:17)
+    Real gravity[3];
+    Real V0;
+    int res[3];
+    int key_bits;           // bits per axis of the page key space
+    int n_materials;
+    MaterialDev<Real> mat[kMaxMaterials];
+    int wall_bc, wall_layers;
+    VelocityConditions<Real> bc;
+    int phase_field;
+    int fp64_svd_fallback;  // precision mode 2
+    Real svd_fallback_ratio;
+    Real mobility;          // scene mobility used by the grid phase-field update (material 0)
+    double dx_d, inv_dx_d;  // binning arithmetic is always FP64
+};
+
+// Counters and flags living in device memory (written by kernels, read by host on demand).
+struct Counters {
+    int n_blocks;
+    int n_grid_blocks;
+    unsigned int flags;
+    int pad;
+    double time;
+    long long substeps;
+};
+
+// ---- SPGrid page keys -----------------------------------------------------
+// The page key of block (bx,by,bz) is offset>>12 of SPGridMask::Linear_Offset:
+// Morton interleave with z in bit 0, y in bit 1, x in bit 2 (SPGridMask.cpp:97-105).
+__host__ __device__ inline uint32_t spread3(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__host__ __device__ inline uint32_t compact3(uint32_t v) {
+    v &= 0x09249249u;
+    v = (v | (v >> 2)) & 0x030c30c3u;
+    v = (v | (v >> 4)) & 0x0300f00fu;
+    v = (v | (v >> 8)) & 0x030000ffu;
+    v = (v | (v >> 16)) & 0x000003ffu;
+    return v;
+}
+__host__ __device__ inline uint32_t page_key(int bx, int by, int bz) {
+    return spread3((uint32_t)bz) | (spread3((uint32_t)by) << 1) | (spread3((uint32_t)bx) << 2);
+}
+__host__ __device__ inline void page_coords(uint32_t key, int& bx, int& by, int& bz) {
+    bz = (int)compact3(key);
+    by = (int)compact3(key >> 1);
+    bx = (int)compact3(key >> 2);
+}
+
+__device__ inline void raise_flag(Counters* c, unsigned int f) { atomicOr(&c->flags, f); }
+
+}  // namespace gmpm

@@ -1,0 +1,125 @@
+// Device-wide exclusive prefix sum (reduce -> scan tile sums -> apply), used
+// for page ranks and cell offsets.  Replaces the reference's recursive block
+// scan and Thrust scans (cuda_kernal_tools.cu:15-203, Transformer_kernal.cu:142-207).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gmpm {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+struct ScanScratch {
+    int32_t* tile_sums;  // capacity: ceil(max_n / kScanTile) + 1
+    int64_t capacity;
+};
+
+template <typename TIn>
+__device__ __forceinline__ void scan_load(const TIn* in, int64_t n, int64_t base, int32_t v[kScanItems]) {
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        const int64_t idx = base + q;
+        v[q] = (idx < n) ? (int32_t)in[idx] : 0;
+    }
+}
+
+__device__ __forceinline__ int32_t block_exclusive_sum(int32_t x, int32_t* total) {
+    __shared__ int32_t warp_sums[kScanThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = (lane < kScanThreads / 32) ? warp_sums[lane] : 0;
+        int32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < kScanThreads / 32) warp_sums[lane] = wi - w;
+        if (lane == kScanThreads / 32 - 1) *total = wi;
+    }
+    __syncthreads();
+    const int32_t r = warp_sums[warp] + incl - x;
+    __syncthreads();
+    return r;
+}
+
+template <typename TIn>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const TIn* __restrict__ in, int64_t n,
+                                                               int32_t* __restrict__ tile_sums) {
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int32_t v[kScanItems];
+    scan_load(in, n, base, v);
+    int32_t s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) s += v[q];
+    __shared__ int32_t tot;
+    block_exclusive_sum(s, &tot);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+// Single CTA: exclusive scan of the tile sums in place, total to *total.
+static __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t* __restrict__ tile_sums, int64_t ntiles,
+                                                              int32_t* __restrict__ total) {
+    __shared__ int32_t chunk_total;
+    int32_t carry = 0;
+    for (int64_t base = 0; base < ntiles; base += kScanTile) {
+        const int64_t b = base + (int64_t)threadIdx.x * kScanItems;
+        int32_t v[kScanItems];
+        scan_load(tile_sums, ntiles, b, v);
+        int32_t s = 0;
+#pragma unroll
+        for (int q = 0; q < kScanItems; ++q) s += v[q];
+        int32_t run = block_exclusive_sum(s, &chunk_total) + carry;
+#pragma unroll
+        for (int q = 0; q < kScanItems; ++q) {
+            if (b + q < ntiles) tile_sums[b + q] = run;
+            run += v[q];
+        }
+        carry += chunk_total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+template <typename TIn>
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const TIn* __restrict__ in, int64_t n,
+                                                              const int32_t* __restrict__ tile_offsets,
+                                                              int32_t* __restrict__ out) {
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int32_t v[kScanItems];
+    scan_load(in, n, base, v);
+    int32_t s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) s += v[q];
+    __shared__ int32_t tot;
+    int32_t run = block_exclusive_sum(s, &tot) + tile_offsets[blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        if (base + q < n) out[base + q] = run;
+        run += v[q];
+    }
+}
+
+// out[i] = sum_{j<i} in[j] for i < n; *total = sum of all.
+template <typename TIn>
+inline void scan_exclusive(const TIn* in, int32_t* out, int64_t n, int32_t* total, ScanScratch s,
+                           cudaStream_t stream) {
+    const int64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    k_scan_reduce<TIn><<<(unsigned)ntiles, kScanThreads, 0, stream>>>(in, n, s.tile_sums);
+    k_scan_tiles<<<1, kScanThreads, 0, stream>>>(s.tile_sums, ntiles, total);
+    k_scan_apply<TIn><<<(unsigned)ntiles, kScanThreads, 0, stream>>>(in, n, s.tile_sums, out);
+}
+
+inline int64_t scan_scratch_elems(int64_t max_n) { return (max_n + kScanTile - 1) / kScanTile + 1; }
+
+}  // namespace gmpm

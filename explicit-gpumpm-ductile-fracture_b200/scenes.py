@@ -1,0 +1,159 @@
+"""Synthetic seeded scenes for the plain-path workloads.
+
+The reference samples its scenes from SDF/OBJ assets that are not shipped
+(LoadSample.cpp:109-176); these scenes stand in for them with the sizes and
+parameters of the benchmark configurations:
+
+* ``notched_bar``  — 16x16x64 cells at dx=1/128, 8 particles per cell
+  (131,072 before the notch), pulled apart at +/-0.5 m/s at both ends.
+* ``plates``       — 4 stacked plates of 256x256x16 cells at dx=1/256, 8 ppc
+  (33,554,432 particles), sphere impactor r=0.1 at 5 m/s, gravity -9.8.
+* ``plates_8m``    — the same scene at 8,388,608 particles: 4 plates of
+  128x128x16 cells at dx=1/128 with 8 ppc.
+
+Material parameters follow the configurations: rho=1000, E=1e5 (per plate
+log-uniform in [5e4, 5e5] for the plate scenes), nu=0.3, yield 200 Pa with
+linear hardening H=0.1E, phase-field length scale L0=2dx, softening onset at
+equivalent plastic strain 0.05 (the reference compares alpha/2 with ps, so
+ps=0.025), and the reference's remaining fracture constants.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from . import gmpm as G
+
+
+@dataclasses.dataclass
+class SceneSpec:
+    name: str
+    desc: G.SceneDesc
+    positions: np.ndarray
+    masses: np.ndarray
+    velocities: np.ndarray
+    material_ids: np.ndarray
+    substeps: int
+
+    @property
+    def n(self) -> int:
+        return len(self.positions)
+
+    def build(self, ctx: G.Context) -> G.Scene:
+        return G.Scene(ctx, self.desc, self.positions, self.masses, self.velocities, self.material_ids)
+
+
+def config_material(m: G.Material, dx: float, E: float = 1e5) -> None:
+    m.youngs_modulus = E
+    m.poisson_ratio = 0.3
+    m.density = 1000.0
+    m.yield_stress = 200.0
+    m.hardening_law = G.HARDENING_LINEAR
+    m.hardening = 0.1 * E
+    m.length_scale = 2.0 * dx
+    m.softening_onset = 0.05 / 2.0
+
+
+def notched_bar(seed: int = 0, precision: int = G.PRECISION_FP32, cells=(16, 16, 64), ppc: int = 8,
+                dx: float = 1.0 / 128, pull: float = 0.5, notch=(1, 4), res: int = 128,
+                substeps: int = 500) -> SceneSpec:
+    """Notched bar along z, gripped over 2 cells at each end and pulled apart."""
+    nx, ny, nz = cells
+    origin = ((res - nx) // 2 * dx, (res - ny) // 2 * dx, (res - nz) // 2 * dx)
+    geom = G.Geometry(kind=0, cells=(nx, ny, nz), ppc=ppc, n_plates=1, gap_cells=0, notch_width=notch[0],
+                      notch_depth=notch[1], dx=dx, origin=origin, seed=seed)
+    pos, mat = G.generate_particles(geom)
+    d = G.reference_defaults(dx, (res, res, res))
+    d.dt = 1e-4
+    d.gravity[0] = d.gravity[1] = d.gravity[2] = 0.0
+    d.particle_volume = dx ** 3 / ppc
+    config_material(d.materials[0], dx)
+    z0, z1 = origin[2], origin[2] + nz * dx
+    d.n_slab_bcs = 2
+    d.slabs[0].axis = 2
+    d.slabs[0].lo, d.slabs[0].hi = 0.0, z0 + 2 * dx
+    d.slabs[0].velocity[2] = -pull
+    d.slabs[1].axis = 2
+    d.slabs[1].lo, d.slabs[1].hi = z1 - 2 * dx, res * dx
+    d.slabs[1].velocity[2] = pull
+    d.precision = precision
+    mass = np.full(len(pos), 1000.0 * d.particle_volume)
+    vel = np.zeros_like(pos)
+    return SceneSpec("notched_bar", d, pos, mass, vel, mat, substeps)
+
+
+def _plate_scene(name: str, cells_xy: int, dx: float, ppc: int, margin: int, gap: int, res_y: int, seed: int,
+                 precision: int, substeps: int) -> SceneSpec:
+    n_plates = 4
+    thick = 16
+    res_xz = cells_xy + 2 * margin
+    origin = (margin * dx, margin * dx, margin * dx)
+    geom = G.Geometry(kind=1, cells=(cells_xy, thick, cells_xy), ppc=ppc, n_plates=n_plates, gap_cells=gap,
+                      notch_width=0, notch_depth=0, dx=dx, origin=origin, seed=seed)
+    pos, mat = G.generate_particles(geom)
+    d = G.reference_defaults(dx, (res_xz, res_y, res_xz))
+    d.dt = 5e-5
+    d.gravity[0], d.gravity[1], d.gravity[2] = 0.0, -9.8, 0.0
+    d.particle_volume = dx ** 3 / ppc
+    rng = np.random.default_rng(seed)
+    Es = np.exp(rng.uniform(np.log(5e4), np.log(5e5), n_plates))
+    d.n_materials = n_plates
+    for k in range(1, n_plates):
+        d.materials[k] = d.materials[0]  # reference constants for every plate
+    for k in range(n_plates):
+        config_material(d.materials[k], dx, float(Es[k]))
+    top = origin[1] + (n_plates * thick + (n_plates - 1) * gap) * dx
+    r = 0.1
+    d.n_sphere_bcs = 1
+    sp = d.spheres[0]
+    sp.center[0] = sp.center[2] = res_xz * dx / 2
+    sp.center[1] = top + r + 2 * dx
+    sp.radius = r
+    sp.velocity[1] = -5.0
+    d.precision = precision
+    mass = np.full(len(pos), 1000.0 * d.particle_volume)
+    vel = np.zeros_like(pos)
+    return SceneSpec(name, d, pos, mass, vel, mat, substeps)
+
+
+def plates(seed: int = 0, precision: int = G.PRECISION_FP32, substeps: int = 2000) -> SceneSpec:
+    """4 plates of 256x256x16 cells at dx=1/256, 8 ppc: 33,554,432 particles."""
+    return _plate_scene("plates_33m", 256, 1.0 / 256, 8, 8, 8, 160, seed, precision, substeps)
+
+
+def plates_8m(seed: int = 0, precision: int = G.PRECISION_FP32, substeps: int = 100) -> SceneSpec:
+    """4 plates of 128x128x16 cells at dx=1/128, 8 ppc: 8,388,608 particles."""
+    return _plate_scene("plates_8m", 128, 1.0 / 128, 8, 8, 4, 96, seed, precision, substeps)
+
+
+def plates_small(cells_xy: int = 32, seed: int = 0, precision: int = G.PRECISION_FP32,
+                 substeps: int = 50) -> SceneSpec:
+    """Scaled-down plate-impact scene with the same parameters (test size)."""
+    dx = 1.0 / 128
+    return _plate_scene(f"plates_{cells_xy}", cells_xy, dx, 8, 8, 4, 96, seed, precision, substeps)
+
+
+def blob(n_side: int = 12, ppc: int = 8, seed: int = 3, precision: int = G.PRECISION_FP32, dx: float = 1.0 / 64,
+         res: int = 64, velocity=(0.3, -0.2, 0.1), spin: float = 2.0) -> SceneSpec:
+    """Free-flying box with translation + rotation, no gravity, no walls or
+    velocity conditions: mass and momentum must be conserved exactly."""
+    origin = ((res - n_side) // 2 * dx,) * 3
+    geom = G.Geometry(kind=2, cells=(n_side, n_side, n_side), ppc=ppc, n_plates=1, gap_cells=0, notch_width=0,
+                      notch_depth=0, dx=dx, origin=origin, seed=seed)
+    pos, mat = G.generate_particles(geom)
+    d = G.reference_defaults(dx, (res, res, res))
+    d.dt = 1e-4
+    d.gravity[0] = d.gravity[1] = d.gravity[2] = 0.0
+    d.wall_bc = 0
+    d.particle_volume = dx ** 3 / ppc
+    config_material(d.materials[0], dx)
+    d.materials[0].yield_stress = 1e9  # elastic
+    d.precision = precision
+    c = pos.mean(axis=0)
+    vel = np.tile(np.asarray(velocity, dtype=np.float64), (len(pos), 1))
+    r = pos - c
+    vel[:, 0] += -spin * r[:, 1]
+    vel[:, 1] += spin * r[:, 0]
+    mass = np.full(len(pos), 1000.0 * d.particle_volume)
+    return SceneSpec("blob", d, pos, mass, vel, mat, 20)

@@ -1,0 +1,330 @@
+/*
+ * gmpm.h — C-ABI of the B200-native explicit MPM ductile-fracture substep.
+ *
+ * The library runs the explicit APIC-MPM substep of
+ * KemengHuang/Explicit-GPUMPM-Ductile-Fracture on a sparse paged grid (SPGrid:
+ * 4x4x4-node pages addressed by Morton-interleaved page keys):
+ *   particle binning by page/cell key  ->  P2G  ->  grid update (gravity,
+ *   walls, velocity conditions, explicit phase-field evolution)  ->  G2P with
+ *   the C-matrix and F update, 3x3 QR/Givens SVD, Hencky plastic return
+ *   mapping with hardening and the plastic-strain-driven damage update.
+ *
+ * Every entry point returns a gmpm_status; nothing calls exit().  The library
+ * owns all device memory; the caller owns host buffers.  One host thread per
+ * context.  Stream arguments are `cudaStream_t` passed as `void*` (NULL = the
+ * legacy default stream).
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the reference project root).
+ */
+#ifndef GMPM_H
+#define GMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GMPM_ABI_VERSION 1
+
+/* Status codes.  Replaces CUDA_SAFE_CALL's print-and-exit(0)
+ * (GPU_MPM/cuda_tools.h:25-36) and unchecked kernel launches. */
+typedef enum gmpm_status {
+    GMPM_OK = 0,
+    GMPM_INVALID_ARG = 1,
+    GMPM_OOM = 2,
+    GMPM_TABLE_OVERFLOW = 3,   /* block/page capacity exceeded (reference: unbounded hash probes) */
+    GMPM_NONFINITE = 4,        /* non-finite particle state detected */
+    GMPM_OUT_OF_DOMAIN = 5,    /* particle stencil left the grid (reference quirk: negative base node) */
+    GMPM_CUDA_ERROR = 6,
+    GMPM_NOT_SUPPORTED = 7,
+    GMPM_NO_DEVICE = 8
+} gmpm_status;
+
+/* Device-side status flags accumulated during substeps (gmpm_diagnostics.flags). */
+#define GMPM_FLAG_OUT_OF_DOMAIN   0x1u
+#define GMPM_FLAG_NONFINITE       0x2u
+#define GMPM_FLAG_SVD_NOCONVERGE  0x4u
+#define GMPM_FLAG_TABLE_OVERFLOW  0x8u
+
+typedef enum gmpm_precision {
+    GMPM_PRECISION_FP32 = 0,          /* FP32 state and arithmetic */
+    GMPM_PRECISION_FP64 = 1,          /* FP64 everywhere (reference precision, Setting.h:3-5) */
+    GMPM_PRECISION_FP32_FP64SVD = 2   /* FP32 bulk; FP64 SVD + return map when sigma_min/sigma_max < svd_fallback_ratio */
+} gmpm_precision;
+
+typedef enum gmpm_hardening {
+    GMPM_HARDENING_EXPONENTIAL = 0,   /* reference R(alpha) (ExplicitTimeIntegrator.cu:64-68) */
+    GMPM_HARDENING_LINEAR = 1         /* R(alpha) = yield + H * alpha */
+} gmpm_hardening;
+
+typedef enum gmpm_phase_field {
+    GMPM_PHASE_FIELD_OFF = 0,
+    GMPM_PHASE_FIELD_EXPLICIT = 1     /* explicit diffusion, pointwise-implicit reaction */
+} gmpm_phase_field;
+
+/* Material and fracture constants.  Replaces ElasticMaterial
+ * (GPU_MPM/Materials.h:15-23, Materials.cpp:4-13) and the constants hard-coded
+ * in applyVonMises (GPU_MPM/ExplicitTimeIntegrator.cu:188-194,320-335). */
+typedef struct gmpm_material {
+    double youngs_modulus;     /* E */
+    double poisson_ratio;      /* nu */
+    double density;            /* rho (informational; particle masses are explicit) */
+    double yield_stress;       /* reference 800 */
+    int32_t hardening_law;     /* gmpm_hardening */
+    int32_t _pad0;
+    double hardening;          /* exponential rate h (reference 3) or linear modulus H */
+    double alpha_cap;          /* alpha_c, reference 1 */
+    double dlambda_cap;        /* reference 100 */
+    double strain_cap;         /* Hencky strain clamp, reference 3 */
+    double psi_cap;            /* psi+ history accepted below this, reference 1e6 */
+    double fracture_energy;    /* G_c0, reference 3 */
+    double softening_onset;    /* ps, softening when alpha/2 > ps; reference 0.01 */
+    double residual_fracture;  /* residual G_c fraction, reference 0.1 */
+    double theta;              /* degradation floor, reference 0.0001f (float) */
+    double length_scale;       /* L0, reference 0.5*dx */
+    double mobility;           /* M, reference 50 (Materials.cpp:13) */
+} gmpm_material;
+
+/* Velocity condition on nodes inside an axis-aligned slab lo <= x[axis] <= hi. */
+typedef struct gmpm_slab_bc {
+    int32_t axis;
+    int32_t _pad0;
+    double lo, hi;
+    double velocity[3];
+} gmpm_slab_bc;
+
+/* Rigid sphere moving at constant velocity; nodes inside take its velocity
+ * (generalises PullGrid_kernal, GPU_MPM/TimeIntegrator.cu:169-261). */
+typedef struct gmpm_sphere_bc {
+    double center[3];          /* at t = 0 */
+    double radius;
+    double velocity[3];
+} gmpm_sphere_bc;
+
+#define GMPM_MAX_SLAB_BCS 4
+#define GMPM_MAX_MATERIALS 8
+#define GMPM_MAX_SPHERE_BCS 2
+
+typedef struct gmpm_scene_desc {
+    double dx;                 /* grid spacing (Setting.h:14) */
+    int32_t grid_res[3];       /* nodes per axis; domain [0, grid_res*dx) */
+    int32_t _pad0;
+    double dt;                 /* fixed substep (Simulator.cpp:172,213) */
+    double gravity[3];         /* reference: (0,-10,0) hard-coded (TimeIntegrator.cu:100) */
+    double particle_volume;    /* V0 (Simulator.cpp:181) */
+    int32_t n_materials;       /* 1..GMPM_MAX_MATERIALS; particles select one by material id */
+    int32_t _pad1;
+    gmpm_material materials[GMPM_MAX_MATERIALS];
+    int32_t wall_bc;           /* 1 = sticky walls (collideWithGround, TimeIntegrator.cu:117-165) */
+    int32_t wall_layers;       /* nodes i <= wall_layers or i > res - wall_layers; reference 4 */
+    int32_t n_slab_bcs;
+    int32_t n_sphere_bcs;
+    gmpm_slab_bc slabs[GMPM_MAX_SLAB_BCS];
+    gmpm_sphere_bc spheres[GMPM_MAX_SPHERE_BCS];
+    int32_t precision;         /* gmpm_precision */
+    int32_t phase_field;       /* gmpm_phase_field */
+    int32_t deterministic;     /* 1 = fixed-order P2G (bitwise reproducible), 0 = atomic fast mode */
+    int32_t block_capacity;    /* max active pages; 0 = derive from the particle count */
+    double svd_fallback_ratio; /* sigma_min/sigma_max threshold for the FP64 fallback (1e-3) */
+} gmpm_scene_desc;
+
+/* Initial particle state.  Replaces the h_pos/h_vel/h_mass arrays handed to
+ * Particles::initialize (GPU_MPM/Particles.cuh:12, Particles.cpp:8-31).
+ * positions/velocities are count x 3 (xyz interleaved), masses count.
+ * count must be below 2^28 (the material id shares the id word). */
+typedef struct gmpm_particle_init {
+    int64_t count;
+    const double* positions;
+    const double* velocities;  /* may be NULL (zero) */
+    const double* masses;
+    const int32_t* material_ids; /* may be NULL (all 0); each < n_materials */
+} gmpm_particle_init;
+
+/* Particle fields for gmpm_read_particles. Matrices are 3x3 column-major
+ * (element (r,c) at r + 3c), as the reference stores d_F / d_B planes. */
+typedef enum gmpm_field {
+    GMPM_FIELD_POSITION = 0,   /* 3 */
+    GMPM_FIELD_VELOCITY = 1,   /* 3 */
+    GMPM_FIELD_F = 2,          /* 9 */
+    GMPM_FIELD_B = 3,          /* 9, APIC affine matrix */
+    GMPM_FIELD_DAMAGE = 4,     /* 1, phase field c (1 = intact) */
+    GMPM_FIELD_ALPHA = 5,      /* 1, equivalent plastic strain */
+    GMPM_FIELD_PSI_MAX = 6,    /* 1, tensile energy history */
+    GMPM_FIELD_STRESS = 7,     /* 6, V0*P*F^T symmetric: xx yy zz xy xz yz */
+    GMPM_FIELD_VOLUME = 8,     /* 1, V0*det F */
+    GMPM_FIELD_FP = 9,         /* 1, fracture driving coefficient */
+    GMPM_FIELD_PF_FLUX = 10,   /* 3, 4 L0^2 V grad(c) carried to the next P2G */
+    GMPM_FIELD_MASS = 11,      /* 1 */
+    GMPM_FIELD_ID = 12,        /* 1, original particle index (int32) */
+    GMPM_FIELD_COUNT = 13
+} gmpm_field;
+
+typedef enum gmpm_dtype {
+    GMPM_DTYPE_F64 = 0,
+    GMPM_DTYPE_F32 = 1,
+    GMPM_DTYPE_I32 = 2
+} gmpm_dtype;
+
+typedef enum gmpm_order {
+    GMPM_ORDER_INTERNAL = 0,   /* current sorted order (what Attribs_Back_Host copies) */
+    GMPM_ORDER_ORIGINAL = 1    /* original particle index order */
+} gmpm_order;
+
+/* Binning arrays for gmpm_read_binning (bit-exact parity with the oracle). */
+typedef enum gmpm_binning_array {
+    GMPM_BIN_COUNTS = 0,       /* int64[4]: n_particles, n_blocks, n_grid_blocks, key_space */
+    GMPM_BIN_PERM = 1,         /* int32[n]: new slot -> previous slot (d_indexTrans) */
+    GMPM_BIN_KEYS = 2,         /* uint32[n]: (page_key << 6) | cell, sorted */
+    GMPM_BIN_BLOCK_KEYS = 3,   /* uint32[n_blocks]: active page keys, ascending */
+    GMPM_BIN_BLOCK_START = 4,  /* int32[n_blocks + 1]: particle range per page */
+    GMPM_BIN_CELL_START = 5,   /* int32[n_blocks * 64 + 1]: particle range per cell */
+    GMPM_BIN_GRID_KEYS = 6,    /* uint32[n_grid_blocks]: pages incl. + neighbours, ascending */
+    GMPM_BIN_ADJ = 7,          /* int32[n_blocks * 8]: grid-block index of page + (i,j,k), slot 4i+2j+k */
+    GMPM_BIN_COUNT = 8
+} gmpm_binning_array;
+
+typedef struct gmpm_diag {
+    double particle_mass;      /* sum m_p */
+    double particle_momentum[3];
+    double grid_mass;          /* sum over nodes after the last P2G */
+    double grid_momentum[3];   /* sum m_i v_i after the last P2G (incl. dt*f) */
+    double kinetic_energy;
+    double max_speed;          /* for CFL dt (Simulator.cpp:200-225) */
+    double min_damage;
+    double time;               /* simulated time */
+    int64_t substeps;
+    int64_t n_particles;
+    int32_t n_blocks;
+    int32_t n_grid_blocks;
+    uint32_t flags;            /* GMPM_FLAG_* accumulated since creation */
+    int32_t _pad0;
+    int64_t kernel_launches;   /* kernels this scene launched since creation */
+} gmpm_diag;
+
+/* Per-stage device time of gmpm_substep_timed, summed over its substeps
+ * (CUDA events on the launching stream). */
+typedef struct gmpm_stage_times {
+    double bin_ms;             /* binning: keys, page tables, counting sort */
+    double p2g_ms;
+    double grid_ms;
+    double g2p_ms;             /* G2P + constitutive update */
+    double total_ms;
+    int64_t substeps;
+} gmpm_stage_times;
+
+typedef struct gmpm_context gmpm_context;
+typedef struct gmpm_scene gmpm_scene;
+
+/* ---- context / scene lifetime -------------------------------------------- */
+
+/* Replaces cudaSetDevice(0) in init_cuda (GPU_MPM/gl_main.cpp:31-37). */
+gmpm_status gmpm_context_create(int device, gmpm_context** out);
+gmpm_status gmpm_context_destroy(gmpm_context* ctx);
+
+/* Reference-default scene: the constants of Setting.h and applyVonMises with a
+ * caller-chosen grid.  Replaces the compile-time configuration
+ * (GPU_MPM/Setting.h:3-38) and the material of MPMSimulator::build
+ * (GPU_MPM/Simulator.cpp:114-116). */
+gmpm_status gmpm_scene_desc_reference_defaults(gmpm_scene_desc* desc, double dx, int res_x, int res_y, int res_z);
+
+/* Replaces MPMSimulator::build (GPU_MPM/Simulator.cpp:76-198): allocation
+ * (MallocDeviceMEM :16-31, Particles_Malloc_MEM, SPGrid_MEM_Malloc,
+ * Transformer_Malloc_MEM), Particles::initialize (Particles.cpp:8-31,
+ * Particle_kernal.cu:441-481), F = I and B = 0 (buildIntegrator :67-74).
+ * Also evaluates the initial stress so the first substep can start at P2G. */
+gmpm_status gmpm_scene_create(gmpm_context* ctx, const gmpm_scene_desc* desc,
+                              const gmpm_particle_init* init, gmpm_scene** out);
+gmpm_status gmpm_scene_destroy(gmpm_scene* scene);
+
+/* ---- stepping ------------------------------------------------------------- */
+
+/* n substeps of fixed dt.  Replaces ExplicitTimeIntegrator::integrate
+ * (GPU_MPM/ExplicitTimeIntegrator.cu:881-994) including
+ * DomainTransformer::rebuild (Transformer.cpp:71-82) and Particles::reorder
+ * (Particle_kernal.cu:544-573).  Asynchronous on `stream`; no host syncs. */
+gmpm_status gmpm_substep(gmpm_scene* scene, int n, void* stream);
+
+/* gmpm_substep with CUDA events between the stages; waits for completion and
+ * returns the device time of each stage.  Replaces the cudaEvent timers of
+ * ExplicitTimeIntegrator::integrate (ExplicitTimeIntegrator.cu:884-994) that
+ * report preprocess and simulation time. */
+gmpm_status gmpm_substep_timed(gmpm_scene* scene, int n, void* stream, gmpm_stage_times* out);
+
+/* Replace the scene's velocity conditions (slabs and moving spheres) from
+ * host memory, asynchronously on `stream` (pass pinned memory to keep the
+ * copy asynchronous).  Counts must not exceed GMPM_MAX_SLAB_BCS /
+ * GMPM_MAX_SPHERE_BCS.  Generalises the time-dependent spheres of
+ * PullGrid_kernal (GPU_MPM/TimeIntegrator.cu:169-261), whose motion the
+ * reference hard-codes in the kernel. */
+gmpm_status gmpm_set_velocity_conditions(gmpm_scene* scene, const gmpm_slab_bc* slabs, int n_slabs,
+                                         const gmpm_sphere_bc* spheres, int n_spheres, void* stream);
+
+/* Binning alone on the current positions (sort + page tables).  Replaces
+ * Particles::sort_by_offsets (Particle_kernal.cu:484-542) followed by
+ * DomainTransformer::rebuild (Transformer.cpp:71-82). */
+gmpm_status gmpm_rebin(gmpm_scene* scene, void* stream);
+
+/* Wait for all work queued on the scene's streams and report accumulated flags
+ * as a status (OUT_OF_DOMAIN / NONFINITE / TABLE_OVERFLOW). */
+gmpm_status gmpm_scene_sync(gmpm_scene* scene);
+
+/* ---- readback ------------------------------------------------------------- */
+
+/* Copy one particle field to `dst` (host or device pointer, `bytes` capacity).
+ * Replaces Particles::Attribs_Back_Host (GPU_MPM/Particles.cpp:33-52). */
+gmpm_status gmpm_read_particles(gmpm_scene* scene, int field, int dtype, int order,
+                                void* dst, size_t bytes, void* stream);
+
+/* Copy one binning array (gmpm_binning_array) to host memory.  Exposes what
+ * the reference keeps in Particles/DomainTransformer device members
+ * (d_indexTrans, cell_id, d_page2particle, d_cell2particle, d_adjPage:
+ * GPU_MPM/Particles.cuh:26-44, Transformer.cuh:35-50). */
+gmpm_status gmpm_read_binning(gmpm_scene* scene, int array, void* dst, size_t bytes);
+
+/* Conservation / CFL diagnostics computed on the device in FP64.  Replaces
+ * Particles::getMaxParticleVel_c (Particle_kernal.cu:421-440) used by
+ * MPMSimulator::computeDt (Simulator.cpp:200-225). */
+gmpm_status gmpm_diagnostics(gmpm_scene* scene, gmpm_diag* out);
+
+const char* gmpm_status_string(gmpm_status status);
+
+/* ---- synthetic scenes (host only, no device needed) ----------------------- */
+
+/* Seeded synthetic particle sets standing in for the reference's
+ * LoadSample::Initial_data / readObj scenes (GPU_MPM/LoadSample.cpp:109-176),
+ * whose assets are absent.  Every cell of the body receives `ppc` particles
+ * placed uniformly at random inside the cell (splitmix64 stream from `seed`),
+ * positions rounded to FP32-representable values so FP32 and FP64 runs start
+ * from the same state.
+ * Kinds: 0 = notched bar: box of cells[0] x cells[1] x cells[2] cells; the
+ *            notch removes the cells with notch_width z-indices centred on
+ *            the mid-length of z and y-index < notch_depth (full x extent);
+ *        1 = stacked plates: n_plates boxes of cells[] stacked along +y with
+ *            gap_cells empty cells between them; material id = plate index;
+ *        2 = box (kind 0 without notch).
+ * Call with positions == NULL to get the count, then with capacity >= count.
+ * material_ids may be NULL. */
+typedef struct gmpm_scene_geometry {
+    int32_t kind;
+    int32_t cells[3];
+    int32_t ppc;
+    int32_t n_plates;
+    int32_t gap_cells;
+    int32_t notch_width;
+    int32_t notch_depth;
+    int32_t _pad0;
+    double dx;
+    double origin[3];          /* lower corner of the first box */
+    uint64_t seed;
+} gmpm_scene_geometry;
+
+gmpm_status gmpm_generate_particles(const gmpm_scene_geometry* geom, int64_t* count,
+                                    double* positions, int32_t* material_ids, int64_t capacity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GMPM_H */

@@ -1,0 +1,72 @@
+/*
+ * ORACLE — test infrastructure only, never the product.
+ *
+ * FP64 CPU restatement of the reference's explicit APIC-MPM substep
+ * (KemengHuang/Explicit-GPUMPM-Ductile-Fracture, GPU_MPM/).  The reference has
+ * no CPU path; this file restates its kernels so tests can check the CUDA
+ * library against it.  Only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline / reference arm may load it.
+ *
+ * Pinning: the SPGrid masks and Linear_Offset, the material constants and the
+ * 3x3 SVD are checked against the reference's own code compiled here
+ * (oracle/_ref/ref_kat, fixtures in tests/golden/).  The remaining kernels
+ * (applyVonMises, P2G_APIC, undateGrid_kernal, collideWithGround, G2P_APIC,
+ * binning) are __global__/__device__-only in the reference and are checked by
+ * invariants and hand-derived identities.
+ */
+#ifndef GMPM_ORACLE_H
+#define GMPM_ORACLE_H
+
+#include <stdint.h>
+#include "gmpm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* SPGrid bit arithmetic. */
+void     orc_masks(uint64_t out[3]);
+uint64_t orc_bit_spread(uint64_t mask, int64_t data);
+uint64_t orc_linear_offset(int i, int j, int k);
+uint64_t orc_packed_add(uint64_t a, uint64_t b);
+int64_t  orc_bit_pack(uint64_t mask, uint64_t data);
+
+/* 3x3 SVD: F row-major in, U/V row-major and S out (F = U diag(S) V^T). */
+void orc_svd3(const double* F_rowmajor, double* U_rowmajor, double* S, double* V_rowmajor);
+
+/* Material constants lambda, mu, kappa (Materials.cpp:4-13). */
+void orc_lame(double E, double nu, double* lambda, double* mu, double* kappa);
+
+/* One applyVonMises update of a single particle.
+ * io[0..8] F col-major, io[9] g, io[10] alpha, io[11] c, io[12] psi_max.
+ * out: [0..8] F, [9] g_new, [10] alpha, [11] psi_max, [12] FP,
+ *      [13..21] contribution V0*P*F^T col-major, [22] V0*det F. */
+void orc_von_mises(const gmpm_material* mat, double V0, const double* io, double* out);
+
+typedef struct orc_scene orc_scene;
+
+orc_scene* orc_scene_create(const gmpm_scene_desc* desc, int64_t n, const double* pos,
+                            const double* vel, const double* mass, const int32_t* mat_ids);
+void orc_scene_destroy(orc_scene* s);
+void orc_set_threads(int n);
+int  orc_get_threads(void);
+
+/* Run n substeps; returns accumulated GMPM_FLAG_* bits. */
+uint32_t orc_substep(orc_scene* s, int n);
+/* Binning only (canonical stable sort by (key, previous slot)). */
+uint32_t orc_rebin(orc_scene* s);
+
+int64_t orc_num_particles(const orc_scene* s);
+int64_t orc_num_blocks(const orc_scene* s);
+int64_t orc_num_grid_blocks(const orc_scene* s);
+
+/* Field copy in the oracle's current (sorted) order; layout as gmpm_field. */
+void orc_get_field(const orc_scene* s, int field, double* out);
+/* Binning array copy; layout and types as gmpm_binning_array. */
+void orc_get_binning(const orc_scene* s, int array, void* out);
+void orc_diagnostics(const orc_scene* s, gmpm_diag* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

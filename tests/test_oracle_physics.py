@@ -1,0 +1,113 @@
+"""Invariants of the oracle itself: conservation, objectivity and elastic
+idempotence of the constitutive update, canonical binning, determinism."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+
+def vm(oracle, mat, V0, F, g=1.0, alpha=0.0, c=1.0, psi=0.0):
+    io = np.zeros(13)
+    io[:9] = F.reshape(3, 3).T.ravel()  # column-major
+    io[9:] = [g, alpha, c, psi]
+    out = np.zeros(23)
+    dp = C.POINTER(C.c_double)
+    oracle.lib().orc_von_mises(C.byref(mat), V0, io.ctypes.data_as(dp), out.ctypes.data_as(dp))
+    return dict(F=out[:9].reshape(3, 3).T, g=out[9], alpha=out[10], psi=out[11], FP=out[12],
+                sigma=out[13:22].reshape(3, 3).T, vol=out[22])
+
+
+@pytest.fixture(scope="module")
+def material(pkg):
+    d = pkg.gmpm.reference_defaults(1.0 / 128, (64, 64, 64))
+    pkg.scenes.config_material(d.materials[0], 1.0 / 128)
+    return d.materials[0]
+
+
+def test_elastic_update_is_identity_on_F(oracle, material):
+    rng = np.random.default_rng(0)
+    for _ in range(50):
+        F = np.eye(3) + 1e-4 * rng.standard_normal((3, 3))  # well inside the 200 Pa yield surface
+        r = vm(oracle, material, 1e-6, F)
+        assert np.allclose(r["F"], F, rtol=0, atol=1e-15)
+        assert r["alpha"] == 0.0
+        assert np.allclose(r["sigma"], r["sigma"].T, rtol=1e-12, atol=1e-20)  # V0 U diag U^T
+
+
+def test_constitutive_update_is_objective(oracle, material):
+    rng = np.random.default_rng(1)
+    for _ in range(50):
+        F = np.eye(3) + 0.05 * rng.standard_normal((3, 3))
+        Q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        if np.linalg.det(Q) < 0:
+            Q[:, 0] *= -1
+        a = vm(oracle, material, 1e-6, F, alpha=0.01, psi=0.1, c=0.9, g=0.8)
+        b = vm(oracle, material, 1e-6, Q @ F, alpha=0.01, psi=0.1, c=0.9, g=0.8)
+        assert np.allclose(b["F"], Q @ a["F"], rtol=1e-9, atol=1e-12)
+        assert np.allclose(b["sigma"], Q @ a["sigma"] @ Q.T, rtol=1e-8, atol=1e-18)
+        for k in ("alpha", "psi", "FP", "vol"):
+            assert np.isclose(a[k], b[k], rtol=1e-9, atol=1e-18), k
+
+
+def test_plastic_update_respects_caps(oracle, material):
+    F = np.diag([1.5, 0.8, 0.9])
+    r = vm(oracle, material, 1e-6, F)
+    assert 0.0 < r["alpha"] <= material.alpha_cap
+    assert np.linalg.det(r["F"]) > 0
+    assert r["FP"] >= 1.0 and r["psi"] >= 0.0
+
+
+def test_blob_conserves_mass_and_momentum(pkg, oracle):
+    sp = pkg.scenes.blob(precision=pkg.gmpm.PRECISION_FP64)
+    o = oracle.OracleScene(sp.desc, sp.positions, sp.masses, sp.velocities, sp.material_ids)
+    d0 = o.diagnostics(pkg.gmpm.Diag)
+    o.substep(20)
+    d = o.diagnostics(pkg.gmpm.Diag)
+    assert d["particle_mass"] == d0["particle_mass"]
+    assert abs(d["grid_mass"] - d0["particle_mass"]) <= 1e-13 * d0["particle_mass"]
+    p0 = np.array(d0["particle_momentum"])
+    for key in ("particle_momentum", "grid_momentum"):
+        assert np.abs(np.array(d[key]) - p0).max() <= 1e-12 * np.abs(p0).max(), key
+
+
+def test_canonical_binning(pkg, oracle):
+    sp = pkg.scenes.notched_bar()
+    o = oracle.OracleScene(sp.desc, sp.positions, sp.masses, sp.velocities, sp.material_ids)
+    o.substep(3)
+    o.rebin()
+    keys = o.binning(2).astype(np.int64)
+    perm = o.binning(1)
+    assert np.all(np.diff(keys) >= 0)
+    same = np.diff(keys) == 0
+    assert np.all(np.diff(perm)[same] > 0)  # stable: equal keys keep previous order
+    assert np.array_equal(np.sort(perm), np.arange(o.n))
+    bk = o.binning(3).astype(np.int64)
+    bs = o.binning(4)
+    cs = o.binning(5)
+    assert np.array_equal(bk, np.unique(keys >> 6))
+    assert bs[0] == 0 and bs[-1] == o.n and np.array_equal(cs[::64], bs)
+    for b in range(len(bk)):
+        seg = keys[bs[b]:bs[b + 1]]
+        assert np.all((seg >> 6) == bk[b])
+        counts = np.bincount(seg & 63, minlength=64)
+        assert np.array_equal(np.diff(cs[b * 64:b * 64 + 65]), counts)
+    # grid pages: actives and their 7 "+" neighbours, and adjacency into them
+    gk = o.binning(6).astype(np.int64)
+    adj = o.binning(7).reshape(-1, 8)
+    L = oracle.lib()
+    for b in range(len(bk)):
+        for d in range(8):
+            off = L.orc_packed_add(int(bk[b]) << 12, L.orc_linear_offset(4 * (d >> 2), 4 * ((d >> 1) & 1), 4 * (d & 1)))
+            assert gk[adj[b, d]] == off >> 12
+
+
+def test_oracle_is_deterministic(pkg, oracle):
+    sp = pkg.scenes.notched_bar()
+    a = oracle.OracleScene(sp.desc, sp.positions, sp.masses, sp.velocities, sp.material_ids)
+    b = oracle.OracleScene(sp.desc, sp.positions, sp.masses, sp.velocities, sp.material_ids)
+    a.substep(5)
+    b.substep(5)
+    for f in range(12):
+        assert np.array_equal(a.field(f), b.field(f)), f
