@@ -149,10 +149,12 @@ __global__ void k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys, cons
 constexpr int kCanonBuf = 4096;
 __global__ void __launch_bounds__(256) k_bin_canon(BinDev bin, const Counters* cnt) {
     __shared__ int32_t buf[kCanonBuf];
+    __shared__ int32_t cs[65];
     const int nb = min(cnt->n_blocks, bin.nb_cap);
     for (int b = blockIdx.x; b < nb; b += gridDim.x) {
-        const int32_t* cs = bin.cell_start + (int64_t)b * 64;
-        const int bs = cs[0], be = cs[64];
+        __syncthreads();
+        for (int q = threadIdx.x; q < 65; q += blockDim.x) cs[q] = bin.cell_start[(int64_t)b * 64 + q];
+        __syncthreads();
         // Process whole cells in windows that fit the buffer.
         int c0 = 0;
         while (c0 < 64) {
@@ -188,8 +190,6 @@ __global__ void __launch_bounds__(256) k_bin_canon(BinDev bin, const Counters* c
             __syncthreads();
             c0 = c1;
         }
-        (void)bs;
-        (void)be;
     }
 }
 

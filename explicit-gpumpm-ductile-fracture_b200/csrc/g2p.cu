@@ -34,10 +34,12 @@ __device__ __forceinline__ void bspline1d_g(R xp, R inv_dx, R* w, R* g) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kG2PThreads)
+__global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
     k_g2p(const SceneDev<R>* __restrict__ sc, const SceneDev<double>* __restrict__ sc64, PState<R> in,
           PState<R> out, PAux<R> aux, BinDev bin, const R* __restrict__ nodes, Counters* cnt) {
-    __shared__ R win[kGridChannels][kWindowNodes];
+    // window of the page: (v0, v1, v2, dc) per node as one 16-byte group, c_new apart
+    __shared__ __align__(16) R win4[kWindowNodes][4];
+    __shared__ R wincn[kWindowNodes];
     const int nb = min(cnt->n_blocks, bin.nb_cap);
     const R dx = sc->dx, inv_dx = sc->inv_dx, dt = sc->dt, V0 = sc->V0;
     const bool fallback = sc->fp64_svd_fallback && sc64 != nullptr;
@@ -54,9 +56,13 @@ __global__ void __launch_bounds__(kG2PThreads)
             const int a = node / 36, bb = (node / 6) % 6, cc = node % 6;
             const int d = ((a >> 2) << 2) | ((bb >> 2) << 1) | (cc >> 2);
             const int g = adj[d];
-            win[ch][node] = (g >= 0) ? nodes[(int64_t)g * kGridChannels * 64 + ch * 64 + (a & 3) * 16 + (bb & 3) * 4 +
-                                             (cc & 3)]
-                                     : R(0);
+            const R val = (g >= 0) ? nodes[(int64_t)g * kGridChannels * 64 + ch * 64 + (a & 3) * 16 + (bb & 3) * 4 +
+                                           (cc & 3)]
+                                   : R(0);
+            if (ch < 4)
+                win4[node][ch] = val;
+            else
+                wincn[node] = val;
         }
         __syncthreads();
         const int bs = bin.cell_start[(int64_t)b * 64], be = bin.cell_start[(int64_t)b * 64 + 64];
@@ -85,8 +91,14 @@ __global__ void __launch_bounds__(kG2PThreads)
                     for (int k = 0; k < 3; ++k) {
                         const R d2 = R(k) * dx - xp[2];
                         const int node = (li + i) * 36 + (lj + j) * 6 + (lk + k);
-                        const R n0 = win[GC_V0][node], n1 = win[GC_V1][node], n2 = win[GC_V2][node];
-                        const R ndc = win[GC_DC][node], ncn = win[GC_CN][node];
+                        R nv[4];
+                        if (sizeof(R) == 4) {
+                            *reinterpret_cast<float4*>(nv) = *reinterpret_cast<const float4*>(&win4[node][0]);
+                        } else {
+                            *reinterpret_cast<double2*>(nv) = *reinterpret_cast<const double2*>(&win4[node][0]);
+                            *reinterpret_cast<double2*>(nv + 2) = *reinterpret_cast<const double2*>(&win4[node][2]);
+                        }
+                        const R n0 = nv[0], n1 = nv[1], n2 = nv[2], ndc = nv[3], ncn = wincn[node];
                         const R w = wxy * wz[k];
                         const R wg[3] = {gxy0 * wz[k], gxy1 * wz[k], wxy * gz[k]};
                         vp[0] += w * n0;
@@ -111,9 +123,21 @@ __global__ void __launch_bounds__(kG2PThreads)
             // damage: irreversible (G2PKernal.cu:359-366)
             const R c_old = in.c[o];
             const R c_new = fmax(fmin(c_old, c_old + dcp), R(0));
-            R xn[3];
+            // Write the transfer results first so they are dead during the SVD.
+            bool finite = true;
 #pragma unroll
-            for (int a = 0; a < 3; ++a) xn[a] = x[a] + vp[a] * dt;
+            for (int a = 0; a < 3; ++a) {
+                const R xn = x[a] + vp[a] * dt;
+                out.x[a][slot] = xn;
+                aux.v[a][slot] = vp[a];
+                finite = finite && isfinite(xn);
+            }
+#pragma unroll
+            for (int q = 0; q < 9; ++q) aux.B[q][slot] = Bn[q];
+            out.c[slot] = c_new;
+            out.m[slot] = in.m[o];
+            const uint32_t idw = in.id[o];
+            out.id[slot] = idw;
             // F <- (I + dt grad v) F  (G2PKernal.cu:372-404)
             R Fo[9];
             {
@@ -132,7 +156,6 @@ __global__ void __launch_bounds__(kG2PThreads)
                     for (int c = 0; c < 3; ++c)
                         Fo[r + 3 * c] = A[r] * Fi[3 * c] + A[r + 3] * Fi[3 * c + 1] + A[r + 6] * Fi[3 * c + 2];
             }
-            const uint32_t idw = in.id[o];
             const int mat = (int)(idw >> 28);
             const MaterialDev<R>& M = sc->mat[mat];
             const R theta = M.theta;
@@ -160,27 +183,17 @@ __global__ void __launch_bounds__(kG2PThreads)
             if (!so.svd_ok) flags |= GMPM_FLAG_SVD_NOCONVERGE;
             const R L0 = M.length_scale;
             const R qs = R(4) * L0 * L0 * so.vol;
-            bool finite = true;
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                out.x[a][slot] = xn[a];
-                aux.v[a][slot] = vp[a];
-                aux.q[a][slot] = qs * gc[a];
-                finite = finite && isfinite(xn[a]);
-            }
+            for (int a = 0; a < 3; ++a) aux.q[a][slot] = qs * gc[a];
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
                 out.F[q][slot] = so.F[q];
-                aux.B[q][slot] = Bn[q];
                 finite = finite && isfinite(so.F[q]);
             }
 #pragma unroll
             for (int q = 0; q < 6; ++q) aux.sigma[q][slot] = so.sigma[q];
-            out.c[slot] = c_new;
             out.alpha[slot] = so.alpha;
             out.psi[slot] = so.psi;
-            out.m[slot] = in.m[o];
-            out.id[slot] = idw;
             aux.vol[slot] = so.vol;
             aux.FP[slot] = so.FP;
             if (!finite) flags |= GMPM_FLAG_NONFINITE;

@@ -13,13 +13,17 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     return float(num / den) if den > 0 else float(num)
 
 
-def errors(G, gpu, orc, x0: np.ndarray, fields=COMPARED) -> dict:
-    """Relative L2 error per field (positions as displacement from x0)."""
+def errors(G, gpu, orc, x0: np.ndarray, fields=COMPARED, dx: float | None = None) -> dict:
+    """Relative L2 error per field (positions as displacement from x0).  With
+    dx given, also 'position_dx': the largest position difference in grid
+    cells, which stays meaningful when displacements are tiny."""
     out = {}
     for f in fields:
         a = gpu.read(f, order=G.ORDER_ORIGINAL)
         b = orc.field_by_id(G.FIELD[f])
         if f == "position":
+            if dx is not None:
+                out["position_dx"] = float(np.abs(a - b).max() / dx)
             a, b = a - x0, b - x0
         out[f] = rel_l2(a, b)
     return out
