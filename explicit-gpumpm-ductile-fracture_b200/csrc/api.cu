@@ -204,6 +204,7 @@ struct SceneBase {
     virtual gmpm_status read_binning(int array, void* dst, size_t bytes) = 0;
     virtual gmpm_status diagnostics(gmpm_diag* out) = 0;
     virtual gmpm_status sync() = 0;
+    virtual gmpm_status set_dt(double dt, cudaStream_t s) = 0;
     virtual gmpm_status set_velocity_conditions(const gmpm_slab_bc* slabs, int ns, const gmpm_sphere_bc* spheres,
                                                 int nsp, cudaStream_t s) = 0;
 };
@@ -237,6 +238,9 @@ struct Scene : SceneBase {
         for (void* p : allocs) cudaFree(p);
         if (staging) cudaFree(staging);
         if (bc_staging) cudaFreeHost(bc_staging);
+        if (dt_staging) cudaFreeHost(dt_staging);
+        for (cudaEvent_t e : dt_done)
+            if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : bc_done)
             if (e) cudaEventDestroy(e);
     }
@@ -432,8 +436,8 @@ struct Scene : SceneBase {
         if (ev) GMPM_TRY(cudaEventRecord(ev[1], s));
         GMPM_TRY(launch_grid<R>(d_sc, bin, grid, d_cnt, cfg(), s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[2], s));
-        GMPM_TRY(launch_g2p<R>(d_sc, desc.precision == GMPM_PRECISION_FP32_FP64SVD ? d_sc64 : nullptr, st[cur],
-                               st[1 - cur], aux, bin, grid, d_cnt, cfg(), s, desc.dt));
+        GMPM_TRY(launch_g2p<R>(d_sc, d_sc64, desc.precision == GMPM_PRECISION_FP32_FP64SVD ? d_sc64 : nullptr,
+                               st[cur], st[1 - cur], aux, bin, grid, d_cnt, cfg(), s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[3], s));
         launches += 4;  // p2g, grid, g2p, clock advance
         cur = 1 - cur;
@@ -589,6 +593,38 @@ struct Scene : SceneBase {
         out->kernel_launches = launches;
         return GMPM_OK;
     }
+
+    gmpm_status set_dt(double dt, cudaStream_t s) override {
+        if (!(dt > 0)) return GMPM_INVALID_ARG;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        // dt is read by every kernel from the scene block; the 64-bit copy keeps
+        // the FP64-fallback block consistent.  Host staging is pinned and
+        // double-buffered with the velocity conditions' events.
+        if (!dt_staging) GMPM_TRY(cudaMallocHost(reinterpret_cast<void**>(&dt_staging), 2 * sizeof(DtBlock)));
+        if (!dt_done[0]) {
+            GMPM_TRY(cudaEventCreateWithFlags(&dt_done[0], cudaEventDisableTiming));
+            GMPM_TRY(cudaEventCreateWithFlags(&dt_done[1], cudaEventDisableTiming));
+            GMPM_TRY(cudaEventRecord(dt_done[0], s));
+            GMPM_TRY(cudaEventRecord(dt_done[1], s));
+        }
+        const int k = dt_next;
+        dt_next ^= 1;
+        GMPM_TRY(cudaEventSynchronize(dt_done[k]));
+        dt_staging[k].r = (R)dt;
+        dt_staging[k].d = dt;
+        GMPM_TRY(cudaMemcpyAsync(&d_sc->dt, &dt_staging[k].r, sizeof(R), cudaMemcpyHostToDevice, s));
+        GMPM_TRY(cudaMemcpyAsync(&d_sc64->dt, &dt_staging[k].d, sizeof(double), cudaMemcpyHostToDevice, s));
+        GMPM_TRY(cudaEventRecord(dt_done[k], s));
+        desc.dt = dt;
+        return GMPM_OK;
+    }
+    struct DtBlock {
+        R r;
+        double d;
+    };
+    DtBlock* dt_staging = nullptr;
+    cudaEvent_t dt_done[2] = {nullptr, nullptr};
+    int dt_next = 0;
 
     // Two pinned host staging blocks for velocity-condition updates, so an
     // update can be written while the previous copy is still in flight.
@@ -794,6 +830,11 @@ gmpm_status gmpm_read_particles(gmpm_scene* s, int field, int dtype, int order, 
                                 void* stream) {
     if (!s) return GMPM_INVALID_ARG;
     return s->impl->read_particles(field, dtype, order, dst, bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+gmpm_status gmpm_set_dt(gmpm_scene* s, double dt, void* stream) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->set_dt(dt, reinterpret_cast<cudaStream_t>(stream));
 }
 
 gmpm_status gmpm_set_velocity_conditions(gmpm_scene* s, const gmpm_slab_bc* slabs, int n_slabs,

@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
 }
 
 // Advance the device clock after the substep's last reader of it (the grid kernel).
-__global__ void k_advance_time(Counters* cnt, double dt) {
-    cnt->time += dt;
+__global__ void k_advance_time(Counters* cnt, const double* dt) {
+    cnt->time += *dt;
     cnt->substeps += 1;
 }
 
@@ -217,21 +217,21 @@ template cudaError_t prepare_g2p<float>();
 template cudaError_t prepare_g2p<double>();
 
 template <typename R>
-cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, const PState<R>& in,
-                       const PState<R>& out, const PAux<R>& aux, BinDev bin, GridDev grid, Counters* cnt,
-                       LaunchCfg cfg, cudaStream_t stream, double dt) {
+cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, const SceneDev<double>* fallback64,
+                       const PState<R>& in, const PState<R>& out, const PAux<R>& aux, BinDev bin, GridDev grid,
+                       Counters* cnt, LaunchCfg cfg, cudaStream_t stream) {
     const int ctas = max(1, min(bin.nb_cap, cfg.num_sms * 8));
-    k_g2p<R><<<ctas, kG2PThreads, 0, stream>>>(sc, sc64, in, out, aux, bin, reinterpret_cast<const R*>(grid.nodes),
-                                               cnt);
-    k_advance_time<<<1, 1, 0, stream>>>(cnt, dt);
+    k_g2p<R><<<ctas, kG2PThreads, 0, stream>>>(sc, fallback64, in, out, aux, bin,
+                                               reinterpret_cast<const R*>(grid.nodes), cnt);
+    k_advance_time<<<1, 1, 0, stream>>>(cnt, &sc64->dt);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_g2p<float>(const SceneDev<float>*, const SceneDev<double>*, const PState<float>&,
-                                       const PState<float>&, const PAux<float>&, BinDev, GridDev, Counters*,
-                                       LaunchCfg, cudaStream_t, double);
-template cudaError_t launch_g2p<double>(const SceneDev<double>*, const SceneDev<double>*, const PState<double>&,
-                                        const PState<double>&, const PAux<double>&, BinDev, GridDev, Counters*,
-                                        LaunchCfg, cudaStream_t, double);
+template cudaError_t launch_g2p<float>(const SceneDev<float>*, const SceneDev<double>*, const SceneDev<double>*,
+                                       const PState<float>&, const PState<float>&, const PAux<float>&, BinDev,
+                                       GridDev, Counters*, LaunchCfg, cudaStream_t);
+template cudaError_t launch_g2p<double>(const SceneDev<double>*, const SceneDev<double>*, const SceneDev<double>*,
+                                        const PState<double>&, const PState<double>&, const PAux<double>&, BinDev,
+                                        GridDev, Counters*, LaunchCfg, cudaStream_t);
 
 }  // namespace gmpm

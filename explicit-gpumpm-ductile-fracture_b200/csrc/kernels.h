@@ -45,10 +45,12 @@ template <typename R>
 cudaError_t launch_grid(const SceneDev<R>* sc, BinDev bin, GridDev grid, Counters* cnt, LaunchCfg cfg,
                         cudaStream_t stream);
 
+// sc64: the scene block in FP64 (always given; its dt drives the device
+// clock).  fallback64: FP64 materials for the SVD fallback, or nullptr.
 template <typename R>
-cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, const PState<R>& in,
-                       const PState<R>& out, const PAux<R>& aux, BinDev bin, GridDev grid, Counters* cnt,
-                       LaunchCfg cfg, cudaStream_t stream, double dt);
+cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, const SceneDev<double>* fallback64,
+                       const PState<R>& in, const PState<R>& out, const PAux<R>& aux, BinDev bin, GridDev grid,
+                       Counters* cnt, LaunchCfg cfg, cudaStream_t stream);
 
 // Initial constitutive evaluation (F, c, alpha, psi given; g_old = 1).
 template <typename R>

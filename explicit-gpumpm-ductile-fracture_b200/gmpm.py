@@ -109,6 +109,7 @@ SIGNATURES = {
     "gmpm_scene_destroy": (C.c_int, [C.c_void_p]),
     "gmpm_substep": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "gmpm_substep_timed": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "gmpm_set_dt": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
     "gmpm_set_velocity_conditions": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "gmpm_rebin": (C.c_int, [C.c_void_p, C.c_void_p]),
     "gmpm_scene_sync": (C.c_int, [C.c_void_p]),
@@ -231,6 +232,9 @@ class Scene:
         check(lib().gmpm_substep_timed(self.h, int(n), C.c_void_p(stream) if stream else None, C.byref(t)),
               "substep_timed")
         return t.as_dict()
+
+    def set_dt(self, dt: float, stream: int | None = None) -> None:
+        check(lib().gmpm_set_dt(self.h, float(dt), C.c_void_p(stream) if stream else None), "set_dt")
 
     def set_velocity_conditions(self, slabs=(), spheres=(), stream: int | None = None) -> None:
         """Replace the velocity conditions (sequences of SlabBC / SphereBC)."""

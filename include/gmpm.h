@@ -253,6 +253,11 @@ gmpm_status gmpm_substep(gmpm_scene* scene, int n, void* stream);
  * report preprocess and simulation time. */
 gmpm_status gmpm_substep_timed(gmpm_scene* scene, int n, void* stream, gmpm_stage_times* out);
 
+/* Change the substep size (asynchronous on `stream`).  Serves the CFL time
+ * step of MPMSimulator::computeDt (GPU_MPM/Simulator.cpp:200-225), which the
+ * reference passes to integrate() every frame. */
+gmpm_status gmpm_set_dt(gmpm_scene* scene, double dt, void* stream);
+
 /* Replace the scene's velocity conditions (slabs and moving spheres) from
  * host memory, asynchronously on `stream` (pass pinned memory to keep the
  * copy asynchronous).  Counts must not exceed GMPM_MAX_SLAB_BCS /
