@@ -1,0 +1,166 @@
+// Binning of caller-owned device positions with no device allocation.
+//
+// Some callers cannot allocate device memory on the call path: a host
+// framework that owns and budgets every byte of device memory up front (an
+// engine or a coupled solver that hands this library only views of its own
+// buffers), or a latency-critical loop where cudaMalloc's implicit
+// synchronisation and unpredictable cost are not allowed.  This entry point
+// serves them: inputs and outputs are the caller's device buffers and all
+// scratch lives in one file-scope __device__ array of fixed size, resolved once
+// per device with cudaGetSymbolAddress.
+//
+// The array is shared by every call in the process: calls that overlap on the
+// GPU (different streams, or host threads without ordering) race on it and
+// must be serialised by the caller.  Its contents persist between calls, so
+// everything that must start at zero is cleared on the call's stream first.
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+
+#include "kernels.h"
+#include "scan.cuh"
+
+namespace gmpm {
+
+// Limits (also stated in include/gmpm.h).
+constexpr int64_t kNoAllocMaxParticles = int64_t(1) << 20;   // 1,048,576
+constexpr int kNoAllocMaxRes = 128;                          // nodes per axis -> page coordinates < 32
+constexpr int kNoAllocKeyBits = 5;                           // bits per axis of the page key
+constexpr uint32_t kNoAllocKeySpace = 1u << (3 * kNoAllocKeyBits);  // 32,768 pages: every page of the grid
+constexpr int64_t kNoAllocCells = (int64_t)kNoAllocKeySpace * 64;
+
+// Scratch layout (bytes, each region 256-byte aligned).
+constexpr size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+constexpr size_t kOffCounters = 0;
+constexpr size_t kOffKeys = align256(kOffCounters + sizeof(Counters));
+constexpr size_t kOffPageFlag = align256(kOffKeys + kNoAllocMaxParticles * sizeof(uint32_t));
+constexpr size_t kOffPageRank = align256(kOffPageFlag + kNoAllocKeySpace);
+constexpr size_t kOffBlockKeys = align256(kOffPageRank + kNoAllocKeySpace * sizeof(int32_t));
+constexpr size_t kOffCellCount = align256(kOffBlockKeys + kNoAllocKeySpace * sizeof(uint32_t));
+constexpr size_t kOffCellStart = align256(kOffCellCount + kNoAllocCells * sizeof(int32_t));
+constexpr size_t kOffScanTiles = align256(kOffCellStart + (kNoAllocCells + 1) * sizeof(int32_t));
+constexpr size_t kScanTilesElems = (kNoAllocCells + kScanTile - 1) / kScanTile + 1;
+constexpr size_t kNoAllocScratchBytes = align256(kOffScanTiles + kScanTilesElems * sizeof(int32_t));
+static_assert(kNoAllocScratchBytes == GMPM_NOALLOC_SCRATCH_BYTES, "keep include/gmpm.h in step");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Kernels of bin.cu reused unchanged.
+__global__ void k_compact_keys(uint32_t key_space, const uint8_t* __restrict__ flag, const int32_t* __restrict__ rank,
+                               uint32_t* __restrict__ out, int cap, Counters* cnt);
+__global__ void k_bin_hist(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
+                           int32_t* __restrict__ cell_count, int nb_cap);
+__global__ void k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
+                              const int32_t* __restrict__ cell_start, int32_t* __restrict__ fill,
+                              int32_t* __restrict__ perm, uint32_t* __restrict__ keys_sorted, int nb_cap);
+__global__ void k_bin_canon(BinDev bin, const Counters* cnt);
+
+// Page/cell keys of interleaved xyz positions: the same FP64 arithmetic as
+// the scene binning (cal_cellId, Particle_kernal.cu:158-165).
+__global__ void k_noalloc_keys(int64_t n, const float* __restrict__ pos, double inv_dx, int rx, int ry, int rz,
+                               uint32_t* __restrict__ keys, uint8_t* __restrict__ page_flag, Counters* cnt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int res[3] = {rx, ry, rz};
+    int base[3];
+    bool bad = false;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double t = __dadd_rn(__dmul_rn((double)pos[3 * i + a], inv_dx), 0.5);
+        const int hi = res[a] - 3;
+        if (!(t >= 1.0)) {
+            base[a] = 0;
+            bad = true;
+        } else if (t >= (double)(hi + 2)) {
+            base[a] = hi;
+            bad = true;
+        } else {
+            base[a] = (int)t - 1;
+        }
+    }
+    if (bad) raise_flag(cnt, GMPM_FLAG_OUT_OF_DOMAIN);
+    const uint32_t cell = (uint32_t)(((base[0] & 3) << 4) | ((base[1] & 3) << 2) | (base[2] & 3));
+    const uint32_t pk = page_key(base[0] >> 2, base[1] >> 2, base[2] >> 2);
+    keys[i] = (pk << 6) | cell;
+    page_flag[pk] = 1;
+}
+
+namespace {
+
+// Device address of g_noalloc_scratch per device, resolved on first use.
+constexpr int kMaxDevices = 64;
+unsigned char* g_scratch_ptr[kMaxDevices] = {nullptr};
+std::mutex g_scratch_mutex;
+
+cudaError_t scratch_for_current_device(unsigned char** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_ptr[dev] = reinterpret_cast<unsigned char*>(p);
+    }
+    *out = g_scratch_ptr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace gmpm
+
+extern "C" gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_t n, double dx, int res_x, int res_y,
+                                                  int res_z, int32_t* perm, uint32_t* keys_sorted, void* stream) {
+    using namespace gmpm;
+    if (!positions || !perm || !keys_sorted || n <= 0 || !(dx > 0)) return GMPM_INVALID_ARG;
+    if (n > kNoAllocMaxParticles) return GMPM_INVALID_ARG;
+    const int res[3] = {res_x, res_y, res_z};
+    for (int a = 0; a < 3; ++a)
+        if (res[a] < 8 || res[a] > kNoAllocMaxRes) return GMPM_INVALID_ARG;
+    unsigned char* base = nullptr;
+    if (scratch_for_current_device(&base) != cudaSuccess) {
+        cudaGetLastError();
+        return GMPM_CUDA_ERROR;
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    Counters* cnt = reinterpret_cast<Counters*>(base + kOffCounters);
+    BinDev bin{};
+    bin.n = n;
+    bin.key_space = kNoAllocKeySpace;
+    bin.nb_cap = (int32_t)kNoAllocKeySpace;
+    bin.ng_cap = 0;
+    bin.keys = reinterpret_cast<uint32_t*>(base + kOffKeys);
+    bin.keys_sorted = keys_sorted;
+    bin.perm = perm;
+    bin.page_flag = base + kOffPageFlag;
+    bin.page_rank = reinterpret_cast<int32_t*>(base + kOffPageRank);
+    bin.block_keys = reinterpret_cast<uint32_t*>(base + kOffBlockKeys);
+    bin.cell_count = reinterpret_cast<int32_t*>(base + kOffCellCount);
+    bin.cell_start = reinterpret_cast<int32_t*>(base + kOffCellStart);
+    ScanScratch scan{reinterpret_cast<int32_t*>(base + kOffScanTiles), (int64_t)kScanTilesElems};
+
+    // state left by the previous call: clear what must start at zero
+    cudaMemsetAsync(cnt, 0, sizeof(Counters), s);
+    cudaMemsetAsync(bin.page_flag, 0, kNoAllocKeySpace, s);
+    cudaMemsetAsync(bin.cell_count, 0, kNoAllocCells * sizeof(int32_t), s);
+    const int T = 256;
+    const unsigned gn = (unsigned)((n + T - 1) / T);
+    const unsigned gk = (kNoAllocKeySpace + T - 1) / T;
+    k_noalloc_keys<<<gn, T, 0, s>>>(n, positions, 1.0 / dx, res_x, res_y, res_z, bin.keys, bin.page_flag, cnt);
+    scan_exclusive<uint8_t>(bin.page_flag, bin.page_rank, (int64_t)kNoAllocKeySpace, &cnt->n_blocks, scan, s);
+    k_compact_keys<<<gk, T, 0, s>>>(kNoAllocKeySpace, bin.page_flag, bin.page_rank, bin.block_keys, bin.nb_cap, cnt);
+    k_bin_hist<<<gn, T, 0, s>>>(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap);
+    scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, kNoAllocCells, bin.cell_start + kNoAllocCells, scan, s);
+    cudaMemsetAsync(bin.cell_count, 0, kNoAllocCells * sizeof(int32_t), s);
+    k_bin_scatter<<<gn, T, 0, s>>>(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, perm, keys_sorted,
+                                   bin.nb_cap);
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_bin_canon<<<sms * 4, 256, 0, s>>>(bin, cnt);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? GMPM_OOM : GMPM_CUDA_ERROR;
+    return GMPM_OK;
+}

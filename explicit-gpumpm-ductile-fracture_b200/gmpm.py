@@ -35,6 +35,8 @@ FIELD_COMPONENTS = dict(position=3, velocity=3, F=9, B=9, damage=1, alpha=1, psi
 DTYPE_F64, DTYPE_F32, DTYPE_I32 = 0, 1, 2
 ORDER_INTERNAL, ORDER_ORIGINAL = 0, 1
 BIN = dict(counts=0, perm=1, keys=2, block_keys=3, block_start=4, cell_start=5, grid_keys=6, adj=7)
+NOALLOC_MAX_PARTICLES = 1048576
+NOALLOC_MAX_RES = 128
 
 
 class Material(C.Structure):
@@ -117,6 +119,8 @@ SIGNATURES = {
     "gmpm_read_binning": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     "gmpm_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Diag)]),
     "gmpm_status_string": (C.c_char_p, [C.c_int]),
+    "gmpm_bin_positions_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_int, C.c_int, C.c_int,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]),
     "gmpm_generate_particles": (C.c_int, [C.POINTER(Geometry), C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                           C.POINTER(C.c_int32), C.c_int64]),
 }

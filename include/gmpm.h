@@ -296,6 +296,35 @@ gmpm_status gmpm_diagnostics(gmpm_scene* scene, gmpm_diag* out);
 
 const char* gmpm_status_string(gmpm_status status);
 
+/* ---- binning without device allocation -------------------------------------- */
+
+/* Bins caller-owned device positions (interleaved xyz, FP32) by SPGrid page and
+ * cell into caller-owned device outputs, allocating no device memory.  It has
+ * no counterpart in the reference.  It is for callers that cannot allocate on
+ * the call path: a host framework that owns and budgets all device memory and
+ * hands this library only views of its own buffers, or a latency-critical loop
+ * where cudaMalloc's implicit synchronisation is not allowed.
+ *
+ * Outputs: perm[i] = input index of sorted slot i and keys_sorted[i] =
+ * (page_key << 6) | cell, identical to GMPM_BIN_PERM / GMPM_BIN_KEYS of a scene
+ * holding the same positions in the same order (stable sort by key).
+ * Positions whose stencil leaves the grid are clamped as in the scene binning;
+ * no flag is reported.  The call is asynchronous on `stream`.
+ *
+ * Limits: n <= GMPM_NOALLOC_MAX_PARTICLES and 8 <= res <= GMPM_NOALLOC_MAX_RES
+ * per axis; anything larger returns GMPM_INVALID_ARG before any work.
+ * Scratch: one file-scope __device__ array of GMPM_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until process exit.  All calls share
+ * it: calls that overlap on the GPU (different streams, or threads without
+ * ordering) race and must be serialised by the caller.  The first call on a
+ * device resolves the array's address with cudaGetSymbolAddress; make that
+ * first call before any stream capture. */
+#define GMPM_NOALLOC_MAX_PARTICLES 1048576
+#define GMPM_NOALLOC_MAX_RES 128
+#define GMPM_NOALLOC_SCRATCH_BYTES 21269248
+gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_t n, double dx, int res_x, int res_y, int res_z,
+                                       int32_t* perm, uint32_t* keys_sorted, void* stream);
+
 /* ---- synthetic scenes (host only, no device needed) ----------------------- */
 
 /* Seeded synthetic particle sets standing in for the reference's
