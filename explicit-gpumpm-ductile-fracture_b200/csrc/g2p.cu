@@ -3,22 +3,51 @@
 // substep (applyVonMises, ExplicitTimeIntegrator.cu:132-370) and with the
 // phase-field gradient gather (AxG2P_APIC, G2PKernal.cu:1006-1123).
 //
-// One CTA per particle page: the page's 6x6x6 window of v, dc and c_new is
-// staged in shared memory; one thread per particle then gathers its 3x3x3
-// stencil, updates c (irreversibly), x, F = (I + dt grad v) F, the APIC matrix
-// B, runs the SVD + Hencky return map + damage driving force, and writes the
-// particle in the new sorted order.  Reading the previous order through perm
-// and writing the new order is the reorder the reference does with gathers
-// and D2D copies (Particle_kernal.cu:544-573, TimeIntegrator.cu:459-461).
+// Each CTA walks particle pages in runs of up to 256 sorted slots.  For every
+// page it stages the 6x6x6 window of v, dc and c_new in shared memory; one
+// thread per particle then gathers its 3x3x3 stencil, updates c
+// (irreversibly), x, F = (I + dt grad v) F, the APIC matrix B, runs the SVD +
+// Hencky return map + damage driving force, and writes the particle in the
+// new sorted order.  Reading the previous order through perm and writing the
+// new order is the reorder the reference does with gathers and D2D copies
+// (Particle_kernal.cu:544-573, TimeIntegrator.cu:459-461).
 #include <cstdint>
 
+#include "async_copy.cuh"
 #include "constitutive.cuh"
 #include "kernels.h"
 
 namespace gmpm {
 
-constexpr int kG2PThreads = 256;
+// Work unit: up to kG2PUnit consecutive sorted slots of one page.  A CTA
+// walks its pages (grid-stride) unit by unit with a three-deep software
+// pipeline of asynchronous copies:
+//   unit k+2: perm, sorted keys, the page's adjacency row and key   (meta)
+//   unit k+1: the particles' 17 input words (through perm) and, when the
+//             unit starts a new page, the page's 6x6x6 node window   (data)
+//   unit k  : computed from shared memory
+// so global latency is hidden behind the previous unit's arithmetic.
+constexpr int kG2PUnit = 256;
+constexpr int kG2PMinBlocks = 2;  // resident CTAs per SM (FP32), bounded by registers
+constexpr int kPlanesR = 16;  // x0..2, F0..8, c, alpha, psi, m
 
+template <typename R>
+struct G2PShared {
+    R win4[2][kWindowNodes][4];  // (v0, v1, v2, dc) per window node; 2 page buffers
+    R wincn[2][kWindowNodes];    // c_new per window node
+    R p[2][kPlanesR][kG2PUnit];  // staged particle inputs; 2 unit buffers
+    uint32_t id[2][kG2PUnit];
+    int32_t o[3][kG2PUnit];      // previous slot per unit slot; 3 meta buffers
+    uint32_t key[3][kG2PUnit];
+    int32_t adj[3][8];
+    uint32_t bkey[3];
+    int32_t unit[3][4];          // page, first slot, count (0: none), window buffer
+};
+
+enum : int { P_X = 0, P_F = 3, P_C = 12, P_ALPHA = 13, P_PSI = 14, P_M = 15 };
+
+// quadratic B-spline weights and gradients on nodes base+0..2 along one axis,
+// xp relative to the base node (G2PKernal.cu:257-288)
 template <typename R>
 __device__ __forceinline__ void bspline1d_g(R xp, R inv_dx, R* w, R* g) {
     R d0 = xp * inv_dx;
@@ -33,44 +62,154 @@ __device__ __forceinline__ void bspline1d_g(R xp, R inv_dx, R* w, R* g) {
     g[2] = z * inv_dx;
 }
 
+// Unit sequence of one CTA: its pages blockIdx.x + k gridDim.x, each cut into
+// runs of kG2PUnit slots.  Every thread runs the same iterator.
+struct UnitIter {
+    int page, next, end;      // current page, next run start, page end
+    int nbs, nbe;             // slot range of the following page (loaded one page ahead)
+    __device__ void init(const BinDev& bin, int nb) {
+        page = blockIdx.x;
+        next = end = 0;
+        if (page < nb) {
+            next = bin.cell_start[(int64_t)page * 64];
+            end = bin.cell_start[(int64_t)page * 64 + 64];
+        }
+        preload(bin, nb);
+    }
+    __device__ void preload(const BinDev& bin, int nb) {
+        const int q = page + (int)gridDim.x;
+        nbs = nbe = 0;
+        if (q < nb) {
+            nbs = bin.cell_start[(int64_t)q * 64];
+            nbe = bin.cell_start[(int64_t)q * 64 + 64];
+        }
+    }
+    // Next unit (page, first slot, count); count 0 when the CTA is done.
+    __device__ void step(const BinDev& bin, int nb, int& b, int& s0, int& n) {
+        while (page < nb && next >= end) {
+            page += gridDim.x;
+            next = nbs;
+            end = nbe;
+            if (page < nb) preload(bin, nb);
+        }
+        if (page < nb) {
+            b = page;
+            s0 = next;
+            n = min(kG2PUnit, end - next);
+            next += kG2PUnit;
+        } else {
+            b = -1;
+            s0 = 0;
+            n = 0;
+        }
+    }
+};
+
 template <typename R>
-__global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
+__device__ __forceinline__ void issue_meta(G2PShared<R>& S, int m, int b, int s0, int n, const BinDev& bin) {
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    if (t < n) {
+        cp_async_elem(&S.o[m][t], &bin.perm[s0 + t]);
+        cp_async_elem(&S.key[m][t], &bin.keys_sorted[s0 + t]);
+    }
+    if (t < 8) cp_async_elem(&S.adj[m][t], &bin.adj[(int64_t)b * 8 + t]);
+    if (t == 8) cp_async_elem(&S.bkey[m], &bin.block_keys[b]);
+}
+
+template <typename R>
+__device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int n, bool window, int wbuf,
+                                           const PState<R>& in, const R* __restrict__ nodes) {
+    const int t = threadIdx.x;
+    if (t < n) {
+        const int o = S.o[m][t];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) cp_async_elem(&S.p[buf][P_X + a][t], in.x[a] + o);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) cp_async_elem(&S.p[buf][P_F + q][t], in.F[q] + o);
+        cp_async_elem(&S.p[buf][P_C][t], in.c + o);
+        cp_async_elem(&S.p[buf][P_ALPHA][t], in.alpha + o);
+        cp_async_elem(&S.p[buf][P_PSI][t], in.psi + o);
+        cp_async_elem(&S.p[buf][P_M][t], in.m + o);
+        cp_async_elem(&S.id[buf][t], in.id + o);
+    }
+    if (window) {
+        for (int w = t; w < kGridChannels * kWindowNodes; w += kG2PUnit) {
+            const int ch = w / kWindowNodes;
+            const int node = w - ch * kWindowNodes;
+            const int a = node / 36, bb = (node / 6) % 6, cc = node % 6;
+            const int d = ((a >> 2) << 2) | ((bb >> 2) << 1) | (cc >> 2);
+            const int g = S.adj[m][d];
+            R* dst = (ch < 4) ? &S.win4[wbuf][node][ch] : &S.wincn[wbuf][node];
+            if (g >= 0)
+                cp_async_elem(dst, nodes + (int64_t)g * kGridChannels * 64 + ch * 64 + (a & 3) * 16 + (bb & 3) * 4 +
+                                       (cc & 3));
+            else
+                *dst = R(0);
+        }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
     k_g2p(const SceneDev<R>* __restrict__ sc, const SceneDev<double>* __restrict__ sc64, PState<R> in,
           PState<R> out, PAux<R> aux, BinDev bin, const R* __restrict__ nodes, Counters* cnt) {
-    // window of the page: (v0, v1, v2, dc) per node as one 16-byte group, c_new apart
-    __shared__ __align__(16) R win4[kWindowNodes][4];
-    __shared__ R wincn[kWindowNodes];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    G2PShared<R>& S = *reinterpret_cast<G2PShared<R>*>(smem_raw);
+    const int t = threadIdx.x;
     const int nb = min(cnt->n_blocks, bin.nb_cap);
     const R dx = sc->dx, inv_dx = sc->inv_dx, dt = sc->dt, V0 = sc->V0;
     const bool fallback = sc->fp64_svd_fallback && sc64 != nullptr;
     const R ratio = sc->svd_fallback_ratio;
     unsigned int flags = 0;
 
-    for (int b = blockIdx.x; b < nb; b += gridDim.x) {
-        int bx, by, bz;
-        page_coords(bin.block_keys[b], bx, by, bz);
-        const int32_t* adj = bin.adj + (int64_t)b * 8;
-        for (int w = threadIdx.x; w < kGridChannels * kWindowNodes; w += kG2PThreads) {
-            const int ch = w / kWindowNodes;
-            const int node = w - ch * kWindowNodes;
-            const int a = node / 36, bb = (node / 6) % 6, cc = node % 6;
-            const int d = ((a >> 2) << 2) | ((bb >> 2) << 1) | (cc >> 2);
-            const int g = adj[d];
-            const R val = (g >= 0) ? nodes[(int64_t)g * kGridChannels * 64 + ch * 64 + (a & 3) * 16 + (bb & 3) * 4 +
-                                           (cc & 3)]
-                                   : R(0);
-            if (ch < 4)
-                win4[node][ch] = val;
-            else
-                wincn[node] = val;
-        }
+    // prologue: meta of units 0 and 1, data of unit 0
+    UnitIter it;
+    it.init(bin, nb);
+    int b0, s00, n0, b1, s01, n1;
+    it.step(bin, nb, b0, s00, n0);
+    it.step(bin, nb, b1, s01, n1);
+    if (t == 0) {
+        S.unit[0][0] = b0; S.unit[0][1] = s00; S.unit[0][2] = n0; S.unit[0][3] = 0;
+        S.unit[1][0] = b1; S.unit[1][1] = s01; S.unit[1][2] = n1; S.unit[1][3] = (b1 == b0) ? 0 : 1;
+    }
+    issue_meta(S, 0, b0, s00, n0, bin);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    issue_data(S, 0, 0, n0, n0 > 0, 0, in, nodes);
+    issue_meta(S, 1, b1, s01, n1, bin);
+    cp_async_commit();
+
+    for (int k = 0;; ++k) {
+        cp_async_wait_all();
         __syncthreads();
-        const int bs = bin.cell_start[(int64_t)b * 64], be = bin.cell_start[(int64_t)b * 64 + 64];
-        for (int slot = bs + threadIdx.x; slot < be; slot += kG2PThreads) {
-            const int o = bin.perm[slot];
-            const uint32_t cell = bin.keys_sorted[slot] & 63u;
+        const int m0 = k % 3, m1 = (k + 1) % 3, m2 = (k + 2) % 3;
+        const int u0b = S.unit[m0][0], u0s = S.unit[m0][1], u0n = S.unit[m0][2], u0w = S.unit[m0][3];
+        if (u0n <= 0) break;
+        {
+            // unit k+2: iterator step, descriptor and meta; unit k+1: data
+            int b2, s02, n2;
+            it.step(bin, nb, b2, s02, n2);
+            const int u1b = S.unit[m1][0], u1n = S.unit[m1][2], u1w = S.unit[m1][3];
+            if (t == 0) {
+                S.unit[m2][0] = b2;
+                S.unit[m2][1] = s02;
+                S.unit[m2][2] = n2;
+                S.unit[m2][3] = (b2 == u1b) ? u1w : 1 - u1w;
+            }
+            issue_data(S, m1, (k + 1) & 1, u1n, u1n > 0 && u1b != u0b, u1w, in, nodes);
+            issue_meta(S, m2, b2, s02, n2, bin);
+            cp_async_commit();
+        }
+        if (t < u0n) {
+            const int buf = k & 1;
+            const int slot = u0s + t;
+            int bx, by, bz;
+            page_coords(S.bkey[m0], bx, by, bz);
+            const uint32_t cell = S.key[m0][t] & 63u;
             const int li = (int)(cell >> 4), lj = (int)((cell >> 2) & 3), lk = (int)(cell & 3);
-            const R x[3] = {in.x[0][o], in.x[1][o], in.x[2][o]};
+            const R x[3] = {S.p[buf][P_X][t], S.p[buf][P_X + 1][t], S.p[buf][P_X + 2][t]};
             const R xp[3] = {x[0] - R(4 * bx + li) * dx, x[1] - R(4 * by + lj) * dx, x[2] - R(4 * bz + lk) * dx};
             R wx[3], gx[3], wy[3], gy[3], wz[3], gz[3];
             bspline1d_g(xp[0], inv_dx, wx, gx);
@@ -80,6 +219,8 @@ __global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
             R gv[9], Bn[9], gc[3] = {R(0), R(0), R(0)};
 #pragma unroll
             for (int q = 0; q < 9; ++q) gv[q] = Bn[q] = R(0);
+            const R(*win4)[4] = S.win4[u0w];
+            const R* wincn = S.wincn[u0w];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const R d0 = R(i) * dx - xp[0];
@@ -88,9 +229,9 @@ __global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
                     const R d1 = R(j) * dx - xp[1];
                     const R wxy = wx[i] * wy[j], gxy0 = gx[i] * wy[j], gxy1 = wx[i] * gy[j];
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const R d2 = R(k) * dx - xp[2];
-                        const int node = (li + i) * 36 + (lj + j) * 6 + (lk + k);
+                    for (int kk = 0; kk < 3; ++kk) {
+                        const R d2 = R(kk) * dx - xp[2];
+                        const int node = (li + i) * 36 + (lj + j) * 6 + (lk + kk);
                         R nv[4];
                         if (sizeof(R) == 4) {
                             *reinterpret_cast<float4*>(nv) = *reinterpret_cast<const float4*>(&win4[node][0]);
@@ -99,8 +240,8 @@ __global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
                             *reinterpret_cast<double2*>(nv + 2) = *reinterpret_cast<const double2*>(&win4[node][2]);
                         }
                         const R n0 = nv[0], n1 = nv[1], n2 = nv[2], ndc = nv[3], ncn = wincn[node];
-                        const R w = wxy * wz[k];
-                        const R wg[3] = {gxy0 * wz[k], gxy1 * wz[k], wxy * gz[k]};
+                        const R w = wxy * wz[kk];
+                        const R wg[3] = {gxy0 * wz[kk], gxy1 * wz[kk], wxy * gz[kk]};
                         vp[0] += w * n0;
                         vp[1] += w * n1;
                         vp[2] += w * n2;
@@ -121,7 +262,7 @@ __global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
                 }
             }
             // damage: irreversible (G2PKernal.cu:359-366)
-            const R c_old = in.c[o];
+            const R c_old = S.p[buf][P_C][t];
             const R c_new = fmax(fmin(c_old, c_old + dcp), R(0));
             // Write the transfer results first so they are dead during the SVD.
             bool finite = true;
@@ -135,8 +276,8 @@ __global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
 #pragma unroll
             for (int q = 0; q < 9; ++q) aux.B[q][slot] = Bn[q];
             out.c[slot] = c_new;
-            out.m[slot] = in.m[o];
-            const uint32_t idw = in.id[o];
+            out.m[slot] = S.p[buf][P_M][t];
+            const uint32_t idw = S.id[buf][t];
             out.id[slot] = idw;
             // F <- (I + dt grad v) F  (G2PKernal.cu:372-404)
             R Fo[9];
@@ -147,29 +288,28 @@ __global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
                 A[0] += R(1);
                 A[4] += R(1);
                 A[8] += R(1);
-                R Fi[9];
-#pragma unroll
-                for (int q = 0; q < 9; ++q) Fi[q] = in.F[q][o];
 #pragma unroll
                 for (int r = 0; r < 3; ++r)
 #pragma unroll
                     for (int c = 0; c < 3; ++c)
-                        Fo[r + 3 * c] = A[r] * Fi[3 * c] + A[r + 3] * Fi[3 * c + 1] + A[r + 6] * Fi[3 * c + 2];
+                        Fo[r + 3 * c] = A[r] * S.p[buf][P_F + 3 * c][t] + A[r + 3] * S.p[buf][P_F + 3 * c + 1][t] +
+                                        A[r + 6] * S.p[buf][P_F + 3 * c + 2][t];
             }
             const int mat = (int)(idw >> 28);
             const MaterialDev<R>& M = sc->mat[mat];
             const R theta = M.theta;
             const R g_old = c_old * c_old * (R(1) - theta) + theta;
+            const R alpha_in = S.p[buf][P_ALPHA][t], psi_in = S.p[buf][P_PSI][t];
             StressOut<R> so;
-            von_mises_update<R, R>(M, V0, Fo, g_old, in.alpha[o], c_new, in.psi[o], so);
+            von_mises_update<R, R>(M, V0, Fo, g_old, alpha_in, c_new, psi_in, so);
             if (fallback && so.smin_over_smax < ratio) {
                 // FP64 SVD + return map for ill-conditioned F
                 double Fd[9];
 #pragma unroll
                 for (int q = 0; q < 9; ++q) Fd[q] = (double)Fo[q];
                 StressOut<double> sd;
-                von_mises_update<double, double>(sc64->mat[mat], (double)V0, Fd, (double)g_old,
-                                                 (double)in.alpha[o], (double)c_new, (double)in.psi[o], sd);
+                von_mises_update<double, double>(sc64->mat[mat], (double)V0, Fd, (double)g_old, (double)alpha_in,
+                                                 (double)c_new, (double)psi_in, sd);
 #pragma unroll
                 for (int q = 0; q < 9; ++q) so.F[q] = (R)sd.F[q];
 #pragma unroll
@@ -198,8 +338,8 @@ __global__ void __launch_bounds__(kG2PThreads, sizeof(R) == 4 ? 2 : 1)
             aux.FP[slot] = so.FP;
             if (!finite) flags |= GMPM_FLAG_NONFINITE;
         }
-        __syncthreads();
     }
+    cp_async_wait_all();
     if (flags) raise_flag(cnt, flags);
 }
 
@@ -211,7 +351,7 @@ __global__ void k_advance_time(Counters* cnt, const double* dt) {
 
 template <typename R>
 cudaError_t prepare_g2p() {
-    return cudaSuccess;
+    return cudaFuncSetAttribute(k_g2p<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(G2PShared<R>));
 }
 template cudaError_t prepare_g2p<float>();
 template cudaError_t prepare_g2p<double>();
@@ -220,8 +360,9 @@ template <typename R>
 cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, const SceneDev<double>* fallback64,
                        const PState<R>& in, const PState<R>& out, const PAux<R>& aux, BinDev bin, GridDev grid,
                        Counters* cnt, LaunchCfg cfg, cudaStream_t stream) {
-    const int ctas = max(1, min(bin.nb_cap, cfg.num_sms * 8));
-    k_g2p<R><<<ctas, kG2PThreads, 0, stream>>>(sc, fallback64, in, out, aux, bin,
+    const int per_sm = sizeof(R) == 4 ? kG2PMinBlocks : 1;
+    const int ctas = max(1, min(bin.nb_cap, cfg.num_sms * per_sm));
+    k_g2p<R><<<ctas, kG2PUnit, sizeof(G2PShared<R>), stream>>>(sc, fallback64, in, out, aux, bin,
                                                reinterpret_cast<const R*>(grid.nodes), cnt);
     k_advance_time<<<1, 1, 0, stream>>>(cnt, &sc64->dt);
     return cudaGetLastError();
