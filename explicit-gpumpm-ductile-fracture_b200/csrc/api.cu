@@ -261,7 +261,9 @@ struct Scene : SceneBase {
         ctx = c;
         desc = *d;
         n = init->count;
-        stride = (int64_t)round_up((size_t)n, 64);
+        // Planes are padded so that a bulk copy of a window of previous slots
+        // around any chunk stays inside the allocation.
+        stride = (int64_t)round_up((size_t)n, 64) + kPlanePad;
         GMPM_TRY(cudaSetDevice(ctx->device));
         // key space of the grid (page coordinates incl. the + neighbour page)
         int maxb = 0;
@@ -298,6 +300,7 @@ struct Scene : SceneBase {
             return p;
         };
         for (int b = 0; b < 2; ++b) {
+            st[b].stride = stride;
             for (int a = 0; a < 3; ++a) st[b].x[a] = next();
             for (int q = 0; q < 9; ++q) st[b].F[q] = next();
             st[b].c = next();
@@ -664,6 +667,7 @@ struct Scene : SceneBase {
         GMPM_TRY(cudaDeviceSynchronize());
         Counters h{};
         GMPM_TRY(cudaMemcpy(&h, d_cnt, sizeof(h), cudaMemcpyDeviceToHost));
+        if (h.flags & GMPM_FLAG_COPY_TIMEOUT) return GMPM_CUDA_ERROR;
         if (h.flags & GMPM_FLAG_TABLE_OVERFLOW) return GMPM_TABLE_OVERFLOW;
         if (h.flags & GMPM_FLAG_OUT_OF_DOMAIN) return GMPM_OUT_OF_DOMAIN;
         if (h.flags & GMPM_FLAG_NONFINITE) return GMPM_NONFINITE;

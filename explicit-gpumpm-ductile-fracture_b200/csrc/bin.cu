@@ -145,9 +145,28 @@ __global__ void k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys, cons
 }
 
 // Canonical in-cell order: ascending previous slot.  One CTA per page; the
-// page's slots are ranked in shared memory (cells hold few particles).
+// page's slots are ranked in shared memory (cells hold few particles).  A page
+// above the buffer is done in windows of whole cells; a single cell above the
+// buffer (thousands of particles in one cell, which only a failed state with
+// clamped positions produces) keeps its scatter order and raises
+// GMPM_FLAG_TABLE_OVERFLOW instead of being ranked in quadratic time.
 constexpr int kCanonBuf = 4096;
-__global__ void __launch_bounds__(256) k_bin_canon(BinDev bin, const Counters* cnt) {
+
+__device__ __forceinline__ void canon_window(const BinDev& bin, const int32_t* cs, int32_t* buf, int lo, int hi) {
+    for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) buf[s - lo] = bin.perm[s];
+    __syncthreads();
+    for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+        const int cell = (int)(bin.keys_sorted[s] & 63);
+        const int a = cs[cell] - lo, e = cs[cell + 1] - lo;
+        const int32_t v = buf[s - lo];
+        int r = 0;
+        for (int u = a; u < e; ++u) r += buf[u] < v;
+        bin.perm[lo + a + r] = v;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_bin_canon(BinDev bin, Counters* cnt) {
     __shared__ int32_t buf[kCanonBuf];
     __shared__ int32_t cs[65];
     const int nb = min(cnt->n_blocks, bin.nb_cap);
@@ -155,39 +174,20 @@ __global__ void __launch_bounds__(256) k_bin_canon(BinDev bin, const Counters* c
         __syncthreads();
         for (int q = threadIdx.x; q < 65; q += blockDim.x) cs[q] = bin.cell_start[(int64_t)b * 64 + q];
         __syncthreads();
-        // Process whole cells in windows that fit the buffer.
+        if (cs[64] - cs[0] <= kCanonBuf) {
+            canon_window(bin, cs, buf, cs[0], cs[64]);
+            continue;
+        }
         int c0 = 0;
         while (c0 < 64) {
             int c1 = c0;
             while (c1 < 64 && cs[c1 + 1] - cs[c0] <= kCanonBuf) ++c1;
             if (c1 == c0) {
-                // A single cell larger than the buffer: rank directly in global
-                // memory using `keys` (free after the scatter) as staging.
-                const int lo = cs[c0], hi = cs[c0 + 1];
-                for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
-                    const int32_t v = bin.perm[s];
-                    int r = 0;
-                    for (int u = lo; u < hi; ++u) r += bin.perm[u] < v;
-                    bin.keys[lo + r] = (uint32_t)v;
-                }
-                __syncthreads();
-                for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) bin.perm[s] = (int32_t)bin.keys[s];
-                __syncthreads();
+                if (threadIdx.x == 0) raise_flag(cnt, GMPM_FLAG_TABLE_OVERFLOW);
                 c0 = c0 + 1;
                 continue;
             }
-            const int lo = cs[c0], hi = cs[c1];
-            for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) buf[s - lo] = bin.perm[s];
-            __syncthreads();
-            for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
-                const int cell = (int)(bin.keys_sorted[s] & 63);
-                const int a = cs[cell] - lo, e = cs[cell + 1] - lo;
-                const int32_t v = buf[s - lo];
-                int r = 0;
-                for (int u = a; u < e; ++u) r += buf[u] < v;
-                bin.perm[lo + a + r] = v;
-            }
-            __syncthreads();
+            canon_window(bin, cs, buf, cs[c0], cs[c1]);
             c0 = c1;
         }
     }

@@ -53,7 +53,7 @@ __global__ void k_bin_hist(int64_t n, const uint32_t* __restrict__ keys, const i
 __global__ void k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
                               const int32_t* __restrict__ cell_start, int32_t* __restrict__ fill,
                               int32_t* __restrict__ perm, uint32_t* __restrict__ keys_sorted, int nb_cap);
-__global__ void k_bin_canon(BinDev bin, const Counters* cnt);
+__global__ void k_bin_canon(BinDev bin, Counters* cnt);
 
 // Page/cell keys of interleaved xyz positions: the same FP64 arithmetic as
 // the scene binning (cal_cellId, Particle_kernal.cu:158-165).

@@ -2,55 +2,95 @@
 // P2GKernal.cu:512-702) plus the phase-field channels (volP2G_APIC,
 // preConditionP2G_APIC, AxP2G_APIC: P2GKernal.cu:897-1326).
 //
-// One CTA per particle page (grid-stride).  A page's particles share the
-// page's 6x6x6 node window and, within a cell, the same 3x3x3 stencil.  The
-// page's particles (sorted by cell) are staged at once (in chunks only for
-// pages above 512 particles), gathered through perm into one 36-word record
-// each in shared memory: x/y offsets, z weights, mass, damage, APIC affine
-// terms, stress and phase-field flux.
+// Each CTA walks its particle pages (grid-stride) in chunks of up to
+// P2GChunk sorted slots (a whole page of 8 particles per cell in FP32).  A
+// page's particles share the page's 6x6x6 node window and, within a cell,
+// the same 3x3x3 stencil.  Between substeps the particle planes are in the
+// previous sorted order and perm is close to the identity, so the 28 raw
+// input planes of the next chunk are fetched as contiguous windows of
+// previous slots with bulk copies (one thread issues them; the tensor memory
+// accelerator moves the data) while the current chunk is swept.  Particles
+// whose previous slot falls outside the window (they changed page) are read
+// directly.  Each thread then turns one particle's raw words into a 44-word
+// record.
 //
-// Work split: 16 cell z-columns (cx, cy) x 9 stencil columns (i, j) x 2
-// channel groups.  Thread (cx, cy, i, j, group) sweeps the cells
-// (cx, cy, 0..3) in order and owns window nodes (cx+i, cy+j, 0..5) for its
-// group's channels: group 0 = momentum x, y + mass + damage weight, group 1 =
-// momentum z + weight + the three phase-field channels.  Every particle of
-// cell cz adds to nodes cz..cz+2 with register indices fixed at compile time
-// (the sweep over cz is unrolled), so the sums stay in registers: no
-// shuffles and no per-particle atomics.
+// Work split: one warp per cell z-column (cx, cy) of the page; lane
+// (g, i, j) = channel group g (0..2) x stencil column (i, j).  A warp sweeps
+// its column's cells (cx, cy, 0..3) in order, all lanes on the same particle,
+// so control flow is uniform.  Lane (g, i, j) owns window nodes
+// (cx+i, cy+j, 0..5) for its group's three channels:
+//   g = 0: momentum x, mass, damage weight
+//   g = 1: momentum y, weight, V w
+//   g = 2: momentum z, V w FP, grad w . q (phase-field flux)
+// Every particle of cell cz adds to nodes cz..cz+2 with register indices
+// fixed at compile time (the sweep over cz is unrolled), so the sums stay in
+// registers: no shuffles and no per-particle atomics.
 //
-// Deterministic mode: the column sums are gathered per window node in a fixed
-// order (at most 9 terms) and written once to the page's tile in HBM, so
-// results are bitwise reproducible.  Fast mode: columns add into a shared
-// tile with atomics.  The grid kernel sums the eight page tiles overlapping
-// each grid page in fixed slot order either way.
+// Deterministic mode: after a page's last chunk the column sums are gathered
+// per window node in a fixed order (at most 9 terms) and written once to the
+// page's tile in HBM, so results are bitwise reproducible.  Fast mode:
+// columns add into a shared tile with atomics.  The grid kernel sums the
+// eight page tiles overlapping each grid page in fixed slot order either way.
 #include <cstdint>
 
+#include "async_copy.cuh"
 #include "kernels.h"
 
 namespace gmpm {
 
-constexpr int kColumns = 144;       // 16 cell z-columns x 9 stencil columns
-constexpr int kGroupThreads = 160;  // 5 warps per channel group (144 busy)
-constexpr int kP2GThreads = 2 * kGroupThreads;
-constexpr int kRec = 36;            // words per staged particle record
-constexpr int kColAcc = 54;         // 6 z-nodes x 9 channels
+constexpr int kP2GWarps = 16;  // one per cell z-column (cx, cy)
+constexpr int kP2GThreads = 32 * kP2GWarps;
+constexpr int kColumns = 144;  // 16 cell z-columns x 9 stencil columns
+constexpr int kColAcc = 54;    // 6 z-nodes x 9 channels per stencil column
+constexpr int kRec = 44;       // words per staged particle record
 
 template <typename R> struct P2GChunk;
 template <> struct P2GChunk<float> { static constexpr int value = 512; };
 template <> struct P2GChunk<double> { static constexpr int value = 256; };
 
-// Staged record layout (words); groups of four are read as 16-byte words.
-enum RecField : int {
-    RF_XP0 = 0, RF_XP1 = 1, RF_M = 2, RF_C = 3,
-    RF_WZ = 4,                  // wz0 wz1 wz2
-    RF_GZ = 7,                  // gz0 gz1 gz2
-    RF_U = 10,                  // m v - m B D^-1 xp          (3)
-    RF_A = 13,                  // dx m B D^-1, (r,c) at 3r+c (9)
-    RF_SXX = 22, RF_SYY = 23, RF_SZZ = 24, RF_SXY = 25, RF_SXZ = 26, RF_SYZ = 27,  // -dt V0 P F^T
-    RF_V = 28, RF_VFP = 29,
-    RF_Q = 30,                  // 4 L0^2 V grad c            (3)
-    RF_PAD = 33
+// Record layout: 8 common words, then one 12-word block per channel group g
+// at RF_BLOCK + 12 g:
+//   U, A0, A1, A2 | S0, S1, S2, s1 | t0, t1, t2, t3
+// with, for a lane of stencil column (i, j) and node k of the sweep,
+//   momentum_g += w (U + A0 i + A1 j + A2 k) + (S0 gxy0 + S1 gxy1) wz + S2 wxy gz
+//   second     += s1 w
+//   third      += (t0 wxy + t1 gxy0 + t2 gxy1) wz + t3 wxy gz
+// where U = m v_g - (m B D^-1 xp)_g, A = dx (m B D^-1) row g, S = -dt V0 P F^T
+// row g.  s1 = (m, 1, V FP); t = (c,0,0,0), (V,0,0,0), (0, q0, q1, q2).
+enum RecField : int { RF_XP0 = 0, RF_XP1 = 1, RF_WZ = 2, RF_GZ = 5, RF_BLOCK = 8 };
+static_assert(RF_BLOCK + 3 * 12 == kRec, "record layout");
+
+// Raw particle planes, in staging order.
+enum RawField : int {
+    RW_X = 0, RW_V = 3, RW_B = 6, RW_SIG = 15, RW_C = 21, RW_M = 22, RW_VOL = 23, RW_FP = 24, RW_Q = 25,
+    kRawWords = 28
 };
+
+// Staging window of previous slots: the chunk's CH slots plus kMargin on
+// either side; planes padded in shared memory to spread banks.
+constexpr int kMargin = 64;
+template <typename R>
+struct Staging {
+    static constexpr int CH = P2GChunk<R>::value;
+    static constexpr int W = CH + 2 * kMargin;             // window length (elements)
+    static constexpr int WS = W + (int)(16 / sizeof(R));   // plane stride in shared memory
+    static_assert(W <= kPlanePad, "window fits the plane padding");
+    static_assert((W * sizeof(R)) % 16 == 0 && (WS * sizeof(R)) % 16 == 0, "bulk copy granularity");
+};
+
+// Device pointer of raw plane q.
+template <typename R>
+__device__ __forceinline__ const R* raw_plane(const PState<R>& st, const PAux<R>& aux, int q) {
+    if (q < RW_V) return st.x[q - RW_X];
+    if (q < RW_B) return aux.v[q - RW_V];
+    if (q < RW_SIG) return aux.B[q - RW_B];
+    if (q < RW_C) return aux.sigma[q - RW_SIG];
+    if (q == RW_C) return st.c;
+    if (q == RW_M) return st.m;
+    if (q == RW_VOL) return aux.vol;
+    if (q == RW_FP) return aux.FP;
+    return aux.q[q - RW_Q];
+}
 
 template <typename R>
 __device__ __forceinline__ void bspline1d(R xp, R inv_dx, R* w, R* g) {
@@ -68,54 +108,65 @@ __device__ __forceinline__ void bspline1d(R xp, R inv_dx, R* w, R* g) {
     g[2] = z * inv_dx;
 }
 
+// Build the particle's record from its raw words.
 template <typename R>
-__device__ __forceinline__ void stage_particle(const SceneDev<R>* __restrict__ sc, const PState<R>& st,
-                                              const PAux<R>& aux, int o, const int base[3], R* rec) {
+__device__ __forceinline__ void build_record(const SceneDev<R>* __restrict__ sc, const int base[3], const R* raw,
+                                             R* rec) {
     const R dx = sc->dx, inv_dx = sc->inv_dx, dt = sc->dt, Dinv = sc->Dinv;
     R xp[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) xp[a] = st.x[a][o] - R(base[a]) * dx;
-    rec[RF_XP0] = xp[0];
-    rec[RF_XP1] = xp[1];
-    {
-        R w[3], g[3];
-        bspline1d(xp[2], inv_dx, w, g);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            rec[RF_WZ + q] = w[q];
-            rec[RF_GZ + q] = g[q];
-        }
-    }
-    const R m = st.m[o];
-    const R V = aux.vol[o];
-    rec[RF_M] = m;
-    rec[RF_C] = st.c[o];
-    rec[RF_V] = V;
-    rec[RF_VFP] = V * aux.FP[o];
+    for (int a = 0; a < 3; ++a) xp[a] = raw[RW_X + a] - R(base[a]) * dx;
+    R out[kRec];
+    out[RF_XP0] = xp[0];
+    out[RF_XP1] = xp[1];
+    bspline1d(xp[2], inv_dx, out + RF_WZ, out + RF_GZ);
+    const R m = raw[RW_M];
+    const R V = raw[RW_VOL];
     R mB[9];  // m B D^-1, (r,c) at 3r+c; B planes are column-major (r + 3c)
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) mB[3 * r + c] = m * aux.B[r + 3 * c][o] * Dinv;
+        for (int c = 0; c < 3; ++c) mB[3 * r + c] = m * raw[RW_B + r + 3 * c] * Dinv;
+    // -dt sigma, sigma stored xx yy zz xy xz yz
+    R S[9];
+    S[0] = -dt * raw[RW_SIG + 0];
+    S[4] = -dt * raw[RW_SIG + 1];
+    S[8] = -dt * raw[RW_SIG + 2];
+    S[1] = S[3] = -dt * raw[RW_SIG + 3];
+    S[2] = S[6] = -dt * raw[RW_SIG + 4];
+    S[5] = S[7] = -dt * raw[RW_SIG + 5];
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        rec[RF_U + r] = m * aux.v[r][o] - (mB[3 * r] * xp[0] + mB[3 * r + 1] * xp[1] + mB[3 * r + 2] * xp[2]);
+    for (int g = 0; g < 3; ++g) {
+        R* blk = out + RF_BLOCK + 12 * g;
+        blk[0] = m * raw[RW_V + g] - (mB[3 * g] * xp[0] + mB[3 * g + 1] * xp[1] + mB[3 * g + 2] * xp[2]);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) rec[RF_A + 3 * r + c] = dx * mB[3 * r + c];
+        for (int c = 0; c < 3; ++c) {
+            blk[1 + c] = dx * mB[3 * g + c];
+            blk[4 + c] = S[3 * g + c];
+        }
     }
-    rec[RF_SXX] = -dt * aux.sigma[0][o];
-    rec[RF_SYY] = -dt * aux.sigma[1][o];
-    rec[RF_SZZ] = -dt * aux.sigma[2][o];
-    rec[RF_SXY] = -dt * aux.sigma[3][o];
-    rec[RF_SXZ] = -dt * aux.sigma[4][o];
-    rec[RF_SYZ] = -dt * aux.sigma[5][o];
+    R* b0 = out + RF_BLOCK;
+    R* b1 = b0 + 12;
+    R* b2 = b1 + 12;
+    b0[7] = m;
+    b0[8] = raw[RW_C];
+    b0[9] = b0[10] = b0[11] = R(0);
+    b1[7] = R(1);
+    b1[8] = V;
+    b1[9] = b1[10] = b1[11] = R(0);
+    b2[7] = V * raw[RW_FP];
+    b2[8] = R(0);
+    b2[9] = raw[RW_Q + 0];
+    b2[10] = raw[RW_Q + 1];
+    b2[11] = raw[RW_Q + 2];
+    static_assert((kRec * sizeof(R)) % 16 == 0, "record must be whole 16-byte words");
 #pragma unroll
-    for (int a = 0; a < 3; ++a) rec[RF_Q + a] = aux.q[a][o];
-    rec[RF_PAD] = rec[RF_PAD + 1] = rec[RF_PAD + 2] = R(0);
+    for (int q = 0; q < (int)(kRec * sizeof(R) / 16); ++q)
+        reinterpret_cast<uint4*>(rec)[q] = reinterpret_cast<const uint4*>(out)[q];
 }
 
-// Per-thread constants of the B-spline piece of stencil node i along one
-// axis, written around z = xp/dx - shift: w = a z^2 + b, dw/dx = c z.
+// Per-lane constants of the B-spline piece of stencil node i along one axis,
+// written around z = xp/dx - shift: w = a z^2 + b, dw/dx = c z.
 template <typename R>
 struct Piece {
     R shift, a, b, c;
@@ -132,150 +183,177 @@ struct Piece {
     }
 };
 
-template <typename R>
-__device__ __forceinline__ void load_record(const R* __restrict__ rec_s, R* rec) {
-    static_assert((kRec * sizeof(R)) % 16 == 0, "record must be whole 16-byte words");
+template <int NW, typename R>
+__device__ __forceinline__ void load_words(const R* __restrict__ src, R* dst) {
+    static_assert((NW * sizeof(R)) % 16 == 0, "whole 16-byte words");
 #pragma unroll
-    for (int q = 0; q < (int)(kRec * sizeof(R) / 16); ++q)
-        reinterpret_cast<uint4*>(rec)[q] = reinterpret_cast<const uint4*>(rec_s)[q];
+    for (int q = 0; q < (int)(NW * sizeof(R) / 16); ++q)
+        reinterpret_cast<uint4*>(dst)[q] = reinterpret_cast<const uint4*>(src)[q];
 }
 
-// Group 0: momentum x, y (incl. dt force), mass, damage weight.
-// acc: 6 z-nodes x {M, P0, P1, CW}.
+// One particle of cell z-index CZ into a lane's 6 z-nodes x 3 channels.
 template <int CZ, typename R>
-__device__ __forceinline__ void accumulate_g0(const R* __restrict__ rec_s, const Piece<R>& px, const Piece<R>& py,
-                                              R inv_dx, R fi, R fj, R* acc) {
-    R rec[kRec];
-    load_record(rec_s, rec);
+__device__ __forceinline__ void accumulate(const R* __restrict__ rec, int g, const Piece<R>& px, const Piece<R>& py,
+                                           R inv_dx, R fi, R fj, R* acc) {
+    R cw[8], bw[12];
+    load_words<8>(rec, cw);
+    load_words<12>(rec + RF_BLOCK + 12 * g, bw);
     R wx, gx, wy, gy;
-    px.eval(rec[RF_XP0] * inv_dx, wx, gx);
-    py.eval(rec[RF_XP1] * inv_dx, wy, gy);
+    px.eval(cw[RF_XP0] * inv_dx, wx, gx);
+    py.eval(cw[RF_XP1] * inv_dx, wy, gy);
     const R wxy = wx * wy, gxy0 = gx * wy, gxy1 = wx * gy;
-    const R mW = rec[RF_M] * wxy, cW = rec[RF_C] * wxy;
-    // dt f_r = (S_r0 gxy0 + S_r1 gxy1) wz + S_r2 wxy gz
-    const R al0 = rec[RF_SXX] * gxy0 + rec[RF_SXY] * gxy1, be0 = rec[RF_SXZ] * wxy;
-    const R al1 = rec[RF_SXY] * gxy0 + rec[RF_SYY] * gxy1, be1 = rec[RF_SYZ] * wxy;
-    R u0 = rec[RF_U + 0] + rec[RF_A + 0] * fi + rec[RF_A + 1] * fj;
-    R u1 = rec[RF_U + 1] + rec[RF_A + 3] * fi + rec[RF_A + 4] * fj;
-    const R a02 = rec[RF_A + 2], a12 = rec[RF_A + 5];
+    const R al = bw[4] * gxy0 + bw[5] * gxy1, be = bw[6] * wxy;
+    const R s1w = bw[7] * wxy;
+    const R gam = bw[8] * wxy + bw[9] * gxy0 + bw[10] * gxy1, del = bw[11] * wxy;
+    R u = bw[0] + bw[1] * fi + bw[2] * fj;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const R wz = rec[RF_WZ + k], gz = rec[RF_GZ + k];
+        const R wz = cw[RF_WZ + k], gz = cw[RF_GZ + k];
         const R w = wxy * wz;
-        R* A = acc + 4 * (CZ + k);
-        A[0] += mW * wz;
-        A[1] += w * u0 + al0 * wz + be0 * gz;
-        A[2] += w * u1 + al1 * wz + be1 * gz;
-        A[3] += cW * wz;
-        u0 += a02;
-        u1 += a12;
+        R* A = acc + 3 * (CZ + k);
+        A[0] += w * u + al * wz + be * gz;
+        A[1] += s1w * wz;
+        A[2] += gam * wz + del * gz;
+        u += bw[3];
     }
 }
 
-// Group 1: momentum z (incl. dt force), weight, V w, V w FP, grad w . q.
-// acc: 6 z-nodes x {P2, W, VW, VWFP, KC}.
 template <int CZ, typename R>
-__device__ __forceinline__ void accumulate_g1(const R* __restrict__ rec_s, const Piece<R>& px, const Piece<R>& py,
-                                              R inv_dx, R fi, R fj, R* acc) {
-    R rec[kRec];
-    load_record(rec_s, rec);
-    R wx, gx, wy, gy;
-    px.eval(rec[RF_XP0] * inv_dx, wx, gx);
-    py.eval(rec[RF_XP1] * inv_dx, wy, gy);
-    const R wxy = wx * wy, gxy0 = gx * wy, gxy1 = wx * gy;
-    const R VW = rec[RF_V] * wxy, FW = rec[RF_VFP] * wxy;
-    const R al2 = rec[RF_SXZ] * gxy0 + rec[RF_SYZ] * gxy1, be2 = rec[RF_SZZ] * wxy;
-    const R gam = rec[RF_Q + 0] * gxy0 + rec[RF_Q + 1] * gxy1, del = rec[RF_Q + 2] * wxy;
-    R u2 = rec[RF_U + 2] + rec[RF_A + 6] * fi + rec[RF_A + 7] * fj;
-    const R a22 = rec[RF_A + 8];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const R wz = rec[RF_WZ + k], gz = rec[RF_GZ + k];
-        const R w = wxy * wz;
-        R* A = acc + 5 * (CZ + k);
-        A[0] += w * u2 + al2 * wz + be2 * gz;
-        A[1] += w;
-        A[2] += VW * wz;
-        A[3] += FW * wz;
-        A[4] += gam * wz + del * gz;
-        u2 += a22;
-    }
-}
-
-template <int G, int CZ, typename R>
-__device__ __forceinline__ void sweep_cell(const R* __restrict__ stage, const int* __restrict__ s_cs, int cb, int c0,
-                                           int c1, const Piece<R>& px, const Piece<R>& py, R inv_dx, R fi, R fj,
-                                           R* acc) {
+__device__ __forceinline__ void sweep_cell(const R* __restrict__ recs, const int* __restrict__ s_cs, int cb, int c0,
+                                           int c1, int g, const Piece<R>& px, const Piece<R>& py, R inv_dx, R fi,
+                                           R fj, R* acc) {
     const int lo = max(s_cs[cb + CZ], c0) - c0, hi = min(s_cs[cb + CZ + 1], c1) - c0;
-    for (int p = lo; p < hi; ++p) {
-        if (G == 0)
-            accumulate_g0<CZ>(stage + (size_t)p * kRec, px, py, inv_dx, fi, fj, acc);
-        else
-            accumulate_g1<CZ>(stage + (size_t)p * kRec, px, py, inv_dx, fi, fj, acc);
-    }
+#pragma unroll 4
+    for (int p = lo; p < hi; ++p) accumulate<CZ>(recs + (size_t)p * kRec, g, px, py, inv_dx, fi, fj, acc);
 }
 
-// Channel (CH_*) of slot Q of group G's accumulator row.
-template <int G, int Q>
-struct GroupChannel {
-    static constexpr int value = G == 0 ? (Q == 0 ? CH_M : Q == 1 ? CH_P0 : Q == 2 ? CH_P1 : CH_CW)
-                                        : (Q == 0 ? CH_P2 : Q == 1 ? CH_W : Q == 2 ? CH_VW : Q == 3 ? CH_VWFP : CH_KC);
+// Channel of slot q (0..2) of group g's accumulator row.
+__device__ __forceinline__ int group_channel(int g, int q) {
+    if (q == 0) return CH_P0 + g;
+    if (q == 1) return g == 0 ? CH_M : (g == 1 ? CH_W : CH_VWFP);
+    return g == 0 ? CH_CW : (g == 1 ? CH_VW : CH_KC);
+}
+
+// Chunk sequence of one CTA: its pages blockIdx.x + k gridDim.x, each cut
+// into runs of CH slots.  Every thread runs the same iterator.
+template <int CH>
+struct ChunkIter {
+    int page, next, end;  // current page, next run start, page end
+    int nbs, nbe;         // slot range of the following page (loaded one page ahead)
+    __device__ void init(const BinDev& bin, int nb) {
+        page = blockIdx.x;
+        next = end = 0;
+        if (page < nb) {
+            next = bin.cell_start[(int64_t)page * 64];
+            end = bin.cell_start[(int64_t)page * 64 + 64];
+        }
+        preload(bin, nb);
+    }
+    __device__ void preload(const BinDev& bin, int nb) {
+        const int q = page + (int)gridDim.x;
+        nbs = nbe = 0;
+        if (q < nb) {
+            nbs = bin.cell_start[(int64_t)q * 64];
+            nbe = bin.cell_start[(int64_t)q * 64 + 64];
+        }
+    }
+    // Next chunk (page, first slot, count, last chunk of its page); count 0 when done.
+    __device__ void step(const BinDev& bin, int nb, int& b, int& s0, int& n, int& last) {
+        while (page < nb && next >= end) {
+            page += gridDim.x;
+            next = nbs;
+            end = nbe;
+            if (page < nb) preload(bin, nb);
+        }
+        if (page < nb) {
+            b = page;
+            s0 = next;
+            n = min(CH, end - next);
+            next += CH;
+            last = next >= end;
+        } else {
+            b = -1;
+            s0 = n = last = 0;
+        }
+    }
 };
 
-template <int G, int Q, typename R, bool kDeterministic>
-__device__ __forceinline__ void flush_channel(const R* acc, R* acc_smem, int l, int a, int bb) {
-    constexpr int NG = G == 0 ? 4 : 5;
-    constexpr int ch = GroupChannel<G, Q>::value;
+template <int CH>
+struct P2GMeta {
+    int32_t o[3][CH];     // previous slot per chunk slot; 3 buffers
+    uint32_t key[3][CH];  // sorted key per chunk slot
+    int32_t cs[3][68];    // cell starts of the chunk's page (65 used)
+    uint32_t bkey[3];
+    int32_t chunk[3][4];  // page, first slot, count (0: none), last chunk of page
+    int64_t win[3];       // first previous slot of the chunk's staging window
+    uint64_t bar;         // completion of the staging bulk copies
+    int abort;            // a bounded wait gave up
+};
+
+// Start of the staging window of a chunk: the median over three particles of
+// (previous slot - slot) estimates the chunk's shift between the orders.
+template <typename R, int CH>
+__device__ __forceinline__ int64_t window_start(const int32_t* o, int n, int64_t stride) {
+    const int64_t d0 = o[0], d1 = (int64_t)o[n / 2] - n / 2, d2 = (int64_t)o[n - 1] - (n - 1);
+    const int64_t med = max(min(d0, d1), min(max(d0, d1), d2));
+    int64_t w = (med - kMargin) & ~(int64_t)3;
+    w = min(w, stride - Staging<R>::W);
+    return max(w, (int64_t)0);
+}
+
+// Thread 0: bulk copies of the 28 raw planes over the chunk's window.
+template <typename R, int CH>
+__device__ __forceinline__ void issue_staging(P2GMeta<CH>& S, R* stage, int64_t w0, const PState<R>& st,
+                                              const PAux<R>& aux) {
+    constexpr int W = Staging<R>::W, WS = Staging<R>::WS;
+    fence_proxy_async_shared();
+    mbar_arrive_expect_tx(&S.bar, (unsigned)(kRawWords * W * sizeof(R)));
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-        if (kDeterministic)
-            acc_smem[(size_t)l * kColAcc + c * 9 + ch] = acc[c * NG + Q];
-        else
-            atomicAdd(&acc_smem[ch * kWindowNodes + a * 36 + bb * 6 + c], acc[c * NG + Q]);
+    for (int q = 0; q < kRawWords; ++q)
+        bulk_copy_g2s(stage + (size_t)q * WS, raw_plane(st, aux, q) + w0, (unsigned)(W * sizeof(R)), &S.bar);
+}
+
+template <int CH>
+__device__ __forceinline__ void issue_p2g_meta(P2GMeta<CH>& S, int m, int b, int s0, int n, const BinDev& bin) {
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    for (int p = t; p < n; p += kP2GThreads) {
+        cp_async_elem(&S.o[m][p], &bin.perm[s0 + p]);
+        cp_async_elem(&S.key[m][p], &bin.keys_sorted[s0 + p]);
     }
+    if (t < 65) cp_async_elem(&S.cs[m][t], &bin.cell_start[(int64_t)b * 64 + t]);
+    if (t == 65) cp_async_elem(&S.bkey[m], &bin.block_keys[b]);
 }
 
-// Sweep the z-column over the chunk [c0, c1) for group G.
-template <int G, typename R>
-__device__ __forceinline__ void run_group(const R* __restrict__ stage, const int* __restrict__ s_cs, int cb, int c0,
-                                          int c1, const Piece<R>& px, const Piece<R>& py, R inv_dx, R fi, R fj,
-                                          R* acc) {
-    sweep_cell<G, 0>(stage, s_cs, cb, c0, c1, px, py, inv_dx, fi, fj, acc);
-    sweep_cell<G, 1>(stage, s_cs, cb, c0, c1, px, py, inv_dx, fi, fj, acc);
-    sweep_cell<G, 2>(stage, s_cs, cb, c0, c1, px, py, inv_dx, fi, fj, acc);
-    sweep_cell<G, 3>(stage, s_cs, cb, c0, c1, px, py, inv_dx, fi, fj, acc);
+template <typename R>
+constexpr size_t p2g_rec_bytes() {
+    return sizeof(R) * (size_t)P2GChunk<R>::value * kRec;
 }
-
-// Write group G's column sums (deterministic: to its partial row; fast: into
-// the shared tile).
-template <int G, typename R, bool kDeterministic>
-__device__ __forceinline__ void flush_group(const R* acc, R* acc_smem, int l, int a, int bb) {
-    flush_channel<G, 0, R, kDeterministic>(acc, acc_smem, l, a, bb);
-    flush_channel<G, 1, R, kDeterministic>(acc, acc_smem, l, a, bb);
-    flush_channel<G, 2, R, kDeterministic>(acc, acc_smem, l, a, bb);
-    flush_channel<G, 3, R, kDeterministic>(acc, acc_smem, l, a, bb);
-    if (G == 1) flush_channel<1, 4, R, kDeterministic>(acc, acc_smem, l, a, bb);
+template <typename R>
+constexpr size_t p2g_stage_bytes() {
+    return sizeof(R) * (size_t)kRawWords * Staging<R>::WS;
 }
 
 template <typename R, bool kDeterministic>
-__global__ void __launch_bounds__(kP2GThreads, sizeof(R) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(kP2GThreads, 1)
     k_p2g(const SceneDev<R>* __restrict__ sc, PState<R> st, PAux<R> aux, BinDev bin, R* __restrict__ tile,
-          const Counters* __restrict__ cnt) {
+          Counters* __restrict__ cnt) {
     constexpr int CH = P2GChunk<R>::value;
-    constexpr int NA = 6 * 5;  // accumulator words (group 1 uses all 30, group 0 the first 24)
+    constexpr int W = Staging<R>::W, WS = Staging<R>::WS;
+    static_assert(sizeof(R) * kColumns * kColAcc <= p2g_rec_bytes<R>(), "column sums fit the record buffer");
+    static_assert(sizeof(R) * kP2GChannels * kWindowNodes <= p2g_rec_bytes<R>(), "tile fits the record buffer");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* stage = reinterpret_cast<R*>(smem_raw);          // [CH][kRec]
-    R* acc_smem = stage + (size_t)CH * kRec;             // det: [144][54] column sums; fast: [9][216] tile
-    __shared__ int s_cs[65];
+    R* recs = reinterpret_cast<R*>(smem_raw);                          // [CH][kRec] particle records
+    R* stage = reinterpret_cast<R*>(smem_raw + p2g_rec_bytes<R>());   // [kRawWords][WS] raw planes
+    P2GMeta<CH>& S = *reinterpret_cast<P2GMeta<CH>*>(smem_raw + p2g_rec_bytes<R>() + p2g_stage_bytes<R>());
 
     const int t = threadIdx.x;
-    const int group = t / kGroupThreads;
-    const int l = t - group * kGroupThreads;
-    const bool worker = l < kColumns;
-    const int colcell = l / 9;  // (cx, cy) = (colcell >> 2, colcell & 3)
-    const int col = l - colcell * 9;
-    const int ci = col / 3, cj = col - (col / 3) * 3;
-    const int cb = (colcell >> 2) * 16 + (colcell & 3) * 4;  // first cell (cz = 0) of the z-column
+    const int warp = t >> 5, lane = t & 31;
+    const int le = lane < 27 ? lane : lane - 27;  // lanes 27..31 shadow lanes 0..4 and never flush
+    const int g = le / 9;
+    const int col = le - g * 9;
+    const int ci = col / 3, cj = col - ci * 3;
+    const int cb = (warp >> 2) * 16 + (warp & 3) * 4;  // first cell (cz = 0) of the z-column
     const R inv_dx = sc->inv_dx;
     const R fi = R(ci), fj = R(cj);
     Piece<R> px, py;
@@ -283,82 +361,168 @@ __global__ void __launch_bounds__(kP2GThreads, sizeof(R) == 4 ? 2 : 1)
     py.init(cj, inv_dx);
     const int nb = min(cnt->n_blocks, bin.nb_cap);
 
-    for (int b = blockIdx.x; b < nb; b += gridDim.x) {
-        for (int q = t; q < 65; q += kP2GThreads) s_cs[q] = bin.cell_start[(int64_t)b * 64 + q];
-        if (!kDeterministic)
-            for (int q = t; q < kP2GChannels * kWindowNodes; q += kP2GThreads) acc_smem[q] = R(0);
-        int bx, by, bz;
-        page_coords(bin.block_keys[b], bx, by, bz);
+    // prologue: meta of chunks 0 and 1, staging of chunk 0
+    ChunkIter<CH> it;
+    it.init(bin, nb);
+    {
+        int b0, s0, n0, l0, b1, s1, n1, l1;
+        it.step(bin, nb, b0, s0, n0, l0);
+        it.step(bin, nb, b1, s1, n1, l1);
+        if (t == 0) {
+            S.chunk[0][0] = b0; S.chunk[0][1] = s0; S.chunk[0][2] = n0; S.chunk[0][3] = l0;
+            S.chunk[1][0] = b1; S.chunk[1][1] = s1; S.chunk[1][2] = n1; S.chunk[1][3] = l1;
+            S.abort = 0;
+            mbar_init(&S.bar, 1);
+            mbar_init_fence();
+        }
+        issue_p2g_meta(S, 0, b0, s0, n0, bin);
+        cp_async_commit();
+        cp_async_wait_all();
         __syncthreads();
-        const int bs = s_cs[0], be = s_cs[64];
-        R acc[NA];
+        if (t == 0 && n0 > 0) {
+            S.win[0] = window_start<R, CH>(S.o[0], n0, st.stride);
+            issue_staging(S, stage, S.win[0], st, aux);
+        }
+        issue_p2g_meta(S, 1, b1, s1, n1, bin);
+        cp_async_commit();
+    }
+
+    R acc[18];
 #pragma unroll
-        for (int q = 0; q < NA; ++q) acc[q] = R(0);
-        for (int c0 = bs; c0 < be; c0 += CH) {
-            const int c1 = min(be, c0 + CH);
-            for (int p = t; p < c1 - c0; p += kP2GThreads) {
-                const int slot = c0 + p;
-                const int o = bin.perm[slot];
-                const uint32_t cell = bin.keys_sorted[slot] & 63u;
+    for (int q = 0; q < 18; ++q) acc[q] = R(0);
+
+    for (int k = 0;; ++k) {
+        const int m0 = k % 3, m1 = (k + 1) % 3, m2 = (k + 2) % 3;
+        cp_async_wait_all();
+        const int n0 = S.chunk[m0][2];
+        if (n0 > 0 && !mbar_wait(&S.bar, (unsigned)(k & 1))) S.abort = 1;
+        __syncthreads();
+        if (n0 <= 0 || S.abort) break;
+        const int b0 = S.chunk[m0][0], c0 = S.chunk[m0][1], last0 = S.chunk[m0][3];
+        // records of chunk k from the staged window (or directly for particles outside it)
+        {
+            int bx, by, bz;
+            page_coords(S.bkey[m0], bx, by, bz);
+            const int64_t w0 = S.win[m0];
+            for (int p = t; p < n0; p += kP2GThreads) {
+                const int o = S.o[m0][p];
+                const int64_t r = (int64_t)o - w0;
+                R raw[kRawWords];
+                if (r >= 0 && r < W) {
+#pragma unroll
+                    for (int q = 0; q < kRawWords; ++q) raw[q] = stage[(size_t)q * WS + r];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < kRawWords; ++q) raw[q] = raw_plane(st, aux, q)[o];
+                }
+                const uint32_t cell = S.key[m0][p] & 63u;
                 const int base[3] = {4 * bx + (int)(cell >> 4), 4 * by + (int)((cell >> 2) & 3),
                                      4 * bz + (int)(cell & 3)};
-                stage_particle(sc, st, aux, o, base, stage + (size_t)p * kRec);
-            }
-            __syncthreads();
-            if (worker) {
-                if (group == 0)
-                    run_group<0>(stage, s_cs, cb, c0, c1, px, py, inv_dx, fi, fj, acc);
-                else
-                    run_group<1>(stage, s_cs, cb, c0, c1, px, py, inv_dx, fi, fj, acc);
-            }
-            __syncthreads();
-        }
-        R* out = tile + (int64_t)b * kP2GChannels * kWindowNodes;
-        {
-            const int a = (colcell >> 2) + ci, bb = (colcell & 3) + cj;
-            if (worker) {
-                if (group == 0)
-                    flush_group<0, R, kDeterministic>(acc, acc_smem, l, a, bb);
-                else
-                    flush_group<1, R, kDeterministic>(acc, acc_smem, l, a, bb);
+                build_record(sc, base, raw, recs + (size_t)p * kRec);
             }
         }
         __syncthreads();
+        {
+            // chunk k+1: staging (the buffer is free now); chunk k+2: iterator step, descriptor and meta
+            const int n1 = S.chunk[m1][2];
+            if (t == 0 && n1 > 0) {
+                S.win[m1] = window_start<R, CH>(S.o[m1], n1, st.stride);
+                issue_staging(S, stage, S.win[m1], st, aux);
+            }
+            int b2, s2, n2, l2;
+            it.step(bin, nb, b2, s2, n2, l2);
+            if (t == 0) {
+                S.chunk[m2][0] = b2;
+                S.chunk[m2][1] = s2;
+                S.chunk[m2][2] = n2;
+                S.chunk[m2][3] = l2;
+            }
+            issue_p2g_meta(S, m2, b2, s2, n2, bin);
+            cp_async_commit();
+        }
+        {
+            const int* s_cs = S.cs[m0];
+            const int c1 = c0 + n0;
+            sweep_cell<0>(recs, s_cs, cb, c0, c1, g, px, py, inv_dx, fi, fj, acc);
+            sweep_cell<1>(recs, s_cs, cb, c0, c1, g, px, py, inv_dx, fi, fj, acc);
+            sweep_cell<2>(recs, s_cs, cb, c0, c1, g, px, py, inv_dx, fi, fj, acc);
+            sweep_cell<3>(recs, s_cs, cb, c0, c1, g, px, py, inv_dx, fi, fj, acc);
+        }
+        if (!last0) continue;
+
+        // Page done: column sums -> the page's tile.  The sums go to the
+        // record buffer, which is free once every warp is past its sweep.
+        __syncthreads();
+        R* acc_smem = recs;
+        const int a = (warp >> 2) + ci, bb = (warp & 3) + cj;
+        if (!kDeterministic) {
+            for (int q = t; q < kP2GChannels * kWindowNodes; q += kP2GThreads) acc_smem[q] = R(0);
+            __syncthreads();
+        }
+        if (lane < 27) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int ch = group_channel(g, q);
+#pragma unroll
+                for (int z = 0; z < 6; ++z) {
+                    if (kDeterministic)
+                        acc_smem[(warp * 9 + col) * kColAcc + z * 9 + ch] = acc[3 * z + q];
+                    else
+                        atomicAdd(&acc_smem[ch * kWindowNodes + a * 36 + bb * 6 + z], acc[3 * z + q]);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 18; ++q) acc[q] = R(0);
+        __syncthreads();
+        R* out = tile + (int64_t)b0 * kP2GChannels * kWindowNodes;
         if (kDeterministic) {
             // window node (a, b, c): sum over cell columns (cx, cy) with stencil
-            // column (a - cx, b - cy), in fixed order
-            for (int oi = t; oi < kP2GChannels * kWindowNodes; oi += kP2GThreads) {
-                const int ch = oi / kWindowNodes;
-                const int node = oi - ch * kWindowNodes;
-                const int a = node / 36, bb = (node / 6) % 6, c = node % 6;
-                R sum = R(0);
-                for (int cx = max(0, a - 2); cx <= min(3, a); ++cx)
-                    for (int cy = max(0, bb - 2); cy <= min(3, bb); ++cy) {
-                        const int thr = (cx * 4 + cy) * 9 + (a - cx) * 3 + (bb - cy);
-                        sum += acc_smem[thr * kColAcc + c * 9 + ch];
+            // column (a - cx, b - cy), cx then cy ascending, all channels at once
+            if (t < kWindowNodes) {
+                const int na = t / 36, nbb = (t / 6) % 6, nc = t % 6;
+                R sum[kP2GChannels];
+#pragma unroll
+                for (int ch = 0; ch < kP2GChannels; ++ch) sum[ch] = R(0);
+                for (int cx = max(0, na - 2); cx <= min(3, na); ++cx)
+                    for (int cy = max(0, nbb - 2); cy <= min(3, nbb); ++cy) {
+                        const R* src =
+                            acc_smem + ((cx * 4 + cy) * 9 + (na - cx) * 3 + (nbb - cy)) * kColAcc + nc * 9;
+#pragma unroll
+                        for (int ch = 0; ch < kP2GChannels; ++ch) sum[ch] += src[ch];
                     }
-                out[oi] = sum;
+#pragma unroll
+                for (int ch = 0; ch < kP2GChannels; ++ch) out[ch * kWindowNodes + t] = sum[ch];
             }
         } else {
             for (int oi = t; oi < kP2GChannels * kWindowNodes; oi += kP2GThreads) out[oi] = acc_smem[oi];
         }
-        __syncthreads();
+        // The record buffer is rebuilt only after the next loop-top barrier.
+    }
+    cp_async_wait_all();
+    if (S.abort) {
+        // A staging copy may still be in flight: wait for it (bounded) before
+        // the CTA's shared memory goes away, and report.
+        if (t == 0) {
+            raise_flag(cnt, GMPM_FLAG_COPY_TIMEOUT);
+            mbar_wait(&S.bar, 0u);
+            mbar_wait(&S.bar, 1u);
+        }
     }
 }
 
-template <typename R, bool kDet>
+template <typename R>
 size_t p2g_smem_bytes() {
-    return sizeof(R) * ((size_t)P2GChunk<R>::value * kRec +
-                        (kDet ? (size_t)kColumns * kColAcc : (size_t)kP2GChannels * kWindowNodes));
+    return p2g_rec_bytes<R>() + p2g_stage_bytes<R>() + sizeof(P2GMeta<P2GChunk<R>::value>);
 }
 
 template <typename R>
 cudaError_t prepare_p2g() {
     cudaError_t e = cudaFuncSetAttribute(k_p2g<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)p2g_smem_bytes<R, true>());
+                                         (int)p2g_smem_bytes<R>());
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_p2g<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)p2g_smem_bytes<R, false>());
+                                (int)p2g_smem_bytes<R>());
 }
 template cudaError_t prepare_p2g<float>();
 template cudaError_t prepare_p2g<double>();
@@ -366,13 +530,12 @@ template cudaError_t prepare_p2g<double>();
 template <typename R>
 cudaError_t launch_p2g(const SceneDev<R>* sc, const PState<R>& st, const PAux<R>& aux, BinDev bin, GridDev grid,
                        Counters* cnt, LaunchCfg cfg, cudaStream_t stream) {
-    const int per_sm = sizeof(R) == 4 ? 2 : 1;
-    const int ctas = max(1, min(bin.nb_cap, cfg.num_sms * per_sm));
+    const int ctas = max(1, min(bin.nb_cap, cfg.num_sms));
     R* tile = reinterpret_cast<R*>(grid.tile);
     if (cfg.deterministic)
-        k_p2g<R, true><<<ctas, kP2GThreads, p2g_smem_bytes<R, true>(), stream>>>(sc, st, aux, bin, tile, cnt);
+        k_p2g<R, true><<<ctas, kP2GThreads, p2g_smem_bytes<R>(), stream>>>(sc, st, aux, bin, tile, cnt);
     else
-        k_p2g<R, false><<<ctas, kP2GThreads, p2g_smem_bytes<R, false>(), stream>>>(sc, st, aux, bin, tile, cnt);
+        k_p2g<R, false><<<ctas, kP2GThreads, p2g_smem_bytes<R>(), stream>>>(sc, st, aux, bin, tile, cnt);
     return cudaGetLastError();
 }
 

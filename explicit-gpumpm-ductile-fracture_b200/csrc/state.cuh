@@ -22,8 +22,13 @@ struct PState {
     R* alpha;
     R* psi;
     R* m;
-    uint32_t* id;  // (material << 28) | original index
+    uint32_t* id;    // (material << 28) | original index
+    int64_t stride;  // elements per plane (>= n + kPlanePad), shared by every particle plane
 };
+
+// Padding of every particle plane beyond n, so a window of kPlanePad previous
+// slots can be bulk-copied around any chunk without leaving the allocation.
+constexpr int kPlanePad = 1024;
 
 // Fields that only G2P writes and only the next P2G reads: single-buffered.
 template <typename R>

@@ -22,7 +22,7 @@ OK, INVALID_ARG, OOM, TABLE_OVERFLOW, NONFINITE, OUT_OF_DOMAIN, CUDA_ERROR, NOT_
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "TABLE_OVERFLOW", 4: "NONFINITE", 5: "OUT_OF_DOMAIN",
                 6: "CUDA_ERROR", 7: "NOT_SUPPORTED", 8: "NO_DEVICE"}
 
-FLAG_OUT_OF_DOMAIN, FLAG_NONFINITE, FLAG_SVD_NOCONVERGE, FLAG_TABLE_OVERFLOW = 1, 2, 4, 8
+FLAG_OUT_OF_DOMAIN, FLAG_NONFINITE, FLAG_SVD_NOCONVERGE, FLAG_TABLE_OVERFLOW, FLAG_COPY_TIMEOUT = 1, 2, 4, 8, 16
 
 PRECISION_FP32, PRECISION_FP64, PRECISION_FP32_FP64SVD = 0, 1, 2
 HARDENING_EXPONENTIAL, HARDENING_LINEAR = 0, 1

@@ -47,7 +47,10 @@ typedef enum gmpm_status {
 #define GMPM_FLAG_OUT_OF_DOMAIN   0x1u
 #define GMPM_FLAG_NONFINITE       0x2u
 #define GMPM_FLAG_SVD_NOCONVERGE  0x4u
-#define GMPM_FLAG_TABLE_OVERFLOW  0x8u
+#define GMPM_FLAG_TABLE_OVERFLOW  0x8u   /* page capacity exceeded, or a cell above 4096 particles
+                                            (that cell then keeps a non-canonical order) */
+#define GMPM_FLAG_COPY_TIMEOUT    0x10u  /* an asynchronous copy did not complete within the kernel's bounded
+                                            wait; the kernel stopped early (reported as GMPM_CUDA_ERROR) */
 
 typedef enum gmpm_precision {
     GMPM_PRECISION_FP32 = 0,          /* FP32 state and arithmetic */
