@@ -288,6 +288,70 @@ def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
                 kernels=kernels, dom=dom, peaks=peaks, e2e=e2e, status=status, build_s=build_s, diag=diag)
 
 
+def run_batched(pkg, local_rank: int, steps: int, plain_steps: int, n_scenes: int = 64, seed: int = 0) -> dict:
+    """The batched workload: 64 independent notched bars (10k-500k particles,
+    log-uniform; parameters within +/-50%; FP32 with FP64 SVD fallback).
+    Aggregate particle-substeps/s of the same scenes (a) one at a time through
+    the plain path (each scene's substeps, scene after scene) and (b) advanced
+    together by one autotuned CUDA-graph launch per substep."""
+    import torch
+
+    G = pkg.gmpm
+    dev = torch.device("cuda", local_rank)
+    ctx = G.Context(local_rank)
+    specs = pkg.scenes.notched_bar_batch(n_scenes, seed=seed)
+    total = sum(sp.n for sp in specs)
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    plain = [sp.build(ctx) for sp in specs]
+    for sc in plain:
+        sc.substep(2, sh)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for sc in plain:
+        sc.substep(plain_steps, sh)
+    e1.record(stream)
+    e1.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain_status = max(sc.sync() for sc in plain)
+    for sc in plain:
+        sc.close()
+    del plain
+
+    scenes = [sp.build(ctx) for sp in specs]
+    batch = G.Batch(ctx, scenes, autotune=True, trial_substeps=2)
+    batch.substep(2, sh)
+    tune = batch.info()["n_candidates"] * 2
+    batch.substep(tune + 2, sh)
+    torch.cuda.synchronize(dev)
+    info = batch.info()
+    launches0 = sum(sc.diagnostics()["kernel_launches"] for sc in scenes)
+    with ClockSampler(local_rank) as clocks:
+        clocks.mark("t0")
+        e0.record(stream)
+        batch.substep(steps, sh)
+        e1.record(stream)
+        e1.synchronize()
+        clocks.mark("t1")
+    b_ms = e0.elapsed_time(e1)
+    launches = sum(sc.diagnostics()["kernel_launches"] for sc in scenes) - launches0
+    status = max(sc.sync() for sc in scenes)
+    batch.close()
+    for sc in scenes:
+        sc.close()
+    rate = total * steps / (b_ms / 1e3)
+    plain_rate = total * plain_steps / (plain_ms / 1e3)
+    return dict(value=rate, unit="particle-substeps/s", scenes=n_scenes, particles=total, steps=steps,
+                ms_per_step=b_ms / steps, plain_sequential=dict(value=plain_rate, steps=plain_steps,
+                                                                ms_per_round=plain_ms / plain_steps),
+                speedup_vs_plain=rate / plain_rate, autotune=info, gpu_launches=launches, clocks=clocks.summary(),
+                status=pkg.gmpm.STATUS_NAMES.get(max(status, plain_status), max(status, plain_status)),
+                workload="64 notched bars, 10k-500k particles log-uniform, params +/-50%, pull U[0.2,1.0] m/s, "
+                         "FP32 + FP64 SVD fallback, dx=1/128, 8 ppc")
+
+
 def sizeof_velocity_conditions(dt) -> int:
     # int n_slabs, n_spheres, slab_axis[4]; Real lo[4], hi[4], vel[4][3], c[2][3], r[2], v[2][3]
     r = np.dtype(dt).itemsize
@@ -302,8 +366,10 @@ def main():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="plates_33m", choices=["plates_33m", "plates_8m", "notched_bar"])
+    ap.add_argument("--workload", default="plates_33m",
+                    choices=["plates_33m", "plates_8m", "notched_bar", "batched64"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload object of the line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -330,6 +396,23 @@ def main():
         print(json.dumps(line))
         return
 
+    if args.workload == "batched64":
+        if rank != 0:
+            return
+        import torch
+        torch.cuda.set_device(local_rank)
+        b = run_batched(pkg, local_rank, steps=args.steps, plain_steps=max(5, args.steps // 4))
+        line = dict(metric="particle-substeps/sec", value=b["value"], unit="particle-substeps/s", n_gpus=1,
+                    steps=args.steps, warmup=args.warmup, ms_per_step=b["ms_per_step"], higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+                    config=dict(workload=b["workload"], particles_per_gpu=b["particles"], scenes=b["scenes"],
+                                parallelism="batched scenes, one CUDA graph per substep",
+                                l2="resident state larger than L2 (no flush needed)"),
+                    plain_sequential=b["plain_sequential"], speedup_vs_plain=b["speedup_vs_plain"],
+                    autotune=b["autotune"], gpu_launches=b["gpu_launches"], clocks=b["clocks"], status=b["status"])
+        print(json.dumps(line))
+        return
+
     dist = None
     if world > 1:
         import datetime
@@ -348,6 +431,13 @@ def main():
         oracle = load_oracle()
         r = time_oracle(pkg, oracle, args.workload, steps=50, warmup=1, budget_s=20.0)
         cpu = dict(value=r["value"], unit=r["unit"], cores=r["cores"], kind=r["kind"], sample=r["sample"])
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        b = run_batched(pkg, local_rank, steps=30, plain_steps=6)
+        batched = {k: b[k] for k in ("value", "unit", "scenes", "particles", "steps", "ms_per_step",
+                                     "plain_sequential", "speedup_vs_plain", "gpu_launches", "status", "workload")}
+        batched["autotune"] = {k: b["autotune"][k] for k in ("streams", "n_candidates", "sm_share_small",
+                                                              "sm_share_medium", "sm_share_large", "graph_nodes")}
     if rank == 0:
         sp = res["sp"]
         k = res["kernels"][res["dom"]]
@@ -363,7 +453,7 @@ def main():
                           peak_source=res["peaks"]["source"]),
             kernels=res["kernels"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
             gpu_launches=res["launches"], status=pkg.gmpm.STATUS_NAMES.get(res["status"], res["status"]),
-            n_blocks=res["diag"]["n_blocks"], n_grid_blocks=res["diag"]["n_grid_blocks"])
+            n_blocks=res["diag"]["n_blocks"], n_grid_blocks=res["diag"]["n_grid_blocks"], batched=batched)
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

@@ -9,15 +9,21 @@
 #include <new>
 #include <vector>
 
-#include "kernels.h"
+#include <atomic>
 
-struct gmpm_context {
-    int device;
-    int num_sms;
-    cudaDeviceProp prop;
-};
+#include "kernels.h"
+#include "scene.h"
 
 namespace gmpm {
+
+gmpm_status cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return GMPM_OK;
+    if (e == cudaErrorMemoryAllocation) return GMPM_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return GMPM_NO_DEVICE;
+    return GMPM_CUDA_ERROR;
+}
+
+std::atomic<uint64_t> g_scene_uid{1};
 
 namespace {
 
@@ -26,13 +32,6 @@ namespace {
         cudaError_t e_ = (expr);                         \
         if (e_ != cudaSuccess) return cuda_status(e_);   \
     } while (0)
-
-gmpm_status cuda_status(cudaError_t e) {
-    if (e == cudaSuccess) return GMPM_OK;
-    if (e == cudaErrorMemoryAllocation) return GMPM_OOM;
-    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return GMPM_NO_DEVICE;
-    return GMPM_CUDA_ERROR;
-}
 
 // Gauss-Jordan with the full pivot search of the reference's Inverse()
 // (ExplicitTimeIntegrator.cu:71-129); evaluated once per material on the host.
@@ -194,21 +193,6 @@ inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 }  // namespace
 
-// Common scene interface, implemented per precision.
-struct SceneBase {
-    virtual ~SceneBase() {}
-    virtual gmpm_status substep(int n, cudaStream_t s) = 0;
-    virtual gmpm_status substep_timed(int n, cudaStream_t s, gmpm_stage_times* out) = 0;
-    virtual gmpm_status rebin(cudaStream_t s) = 0;
-    virtual gmpm_status read_particles(int field, int dtype, int order, void* dst, size_t bytes, cudaStream_t s) = 0;
-    virtual gmpm_status read_binning(int array, void* dst, size_t bytes) = 0;
-    virtual gmpm_status diagnostics(gmpm_diag* out) = 0;
-    virtual gmpm_status sync() = 0;
-    virtual gmpm_status set_dt(double dt, cudaStream_t s) = 0;
-    virtual gmpm_status set_velocity_conditions(const gmpm_slab_bc* slabs, int ns, const gmpm_sphere_bc* spheres,
-                                                int nsp, cudaStream_t s) = 0;
-};
-
 template <typename R>
 struct Scene : SceneBase {
     gmpm_context* ctx = nullptr;
@@ -231,6 +215,9 @@ struct Scene : SceneBase {
     std::vector<void*> allocs;
     bool binned = false;  // binning of the current positions is valid
     int64_t launches = 0;  // kernels launched by this scene
+    uint64_t uid_ = g_scene_uid++;
+    int share_ = 0;        // SMs the launch shapes are sized for (0: all)
+    size_t dev_bytes_ = 0;
     // kernels per launch_binning: keys, 3 scans x 3, mark, 2 compactions, links, hist, scatter, canon
     static constexpr int kBinningKernels = 17;
 
@@ -251,11 +238,14 @@ struct Scene : SceneBase {
         cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
         if (e != cudaSuccess) return e;
         allocs.push_back(q);
+        dev_bytes_ += count * sizeof(T) + 16;
         *p = reinterpret_cast<T*>(q);
         return cudaSuccess;
     }
 
-    LaunchCfg cfg() const { return LaunchCfg{ctx->num_sms, desc.deterministic}; }
+    LaunchCfg cfg() const {
+        return LaunchCfg{share_ > 0 ? std::min(share_, ctx->num_sms) : ctx->num_sms, desc.deterministic};
+    }
 
     gmpm_status create(gmpm_context* c, const gmpm_scene_desc* d, const gmpm_particle_init* init) {
         ctx = c;
@@ -293,6 +283,7 @@ struct Scene : SceneBase {
         const size_t id_bytes = round_up((size_t)stride * sizeof(uint32_t), 256);
         GMPM_TRY(cudaMalloc(&pstore, nplanes * plane_bytes + 2 * id_bytes));
         allocs.push_back(pstore);
+        dev_bytes_ += nplanes * plane_bytes + 2 * id_bytes;
         char* base = reinterpret_cast<char*>(pstore);
         auto next = [&]() {
             R* p = reinterpret_cast<R*>(base);
@@ -424,29 +415,52 @@ struct Scene : SceneBase {
     void mark_grid(cudaStream_t s);
 
     gmpm_status do_bin(cudaStream_t s) {
-        GMPM_TRY(launch_binning<R>(d_sc, st[cur], bin, scan, d_cnt, ctx->num_sms, s));
+        GMPM_TRY(launch_binning<R>(d_sc, st[cur], bin, scan, d_cnt, cfg().num_sms, s));
         binned = true;
         return GMPM_OK;
     }
 
-    // One substep; ev (optional) receives events after bin, p2g, grid, g2p.
-    gmpm_status one_substep(cudaStream_t s, cudaEvent_t* ev) {
-        gmpm_status r = do_bin(s);
-        if (r != GMPM_OK) return r;
-        launches += kBinningKernels;
+    // Kernels of one substep from state buffer c; ev (optional) receives
+    // events after bin, p2g, grid, g2p.  Host bookkeeping is left alone.
+    gmpm_status launch_one(cudaStream_t s, int c, cudaEvent_t* ev) {
+        const LaunchCfg lc = cfg();
+        GMPM_TRY(launch_binning<R>(d_sc, st[c], bin, scan, d_cnt, lc.num_sms, s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[0], s));
-        GMPM_TRY(launch_p2g<R>(d_sc, st[cur], aux, bin, grid, d_cnt, cfg(), s));
+        GMPM_TRY(launch_p2g<R>(d_sc, st[c], aux, bin, grid, d_cnt, lc, s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[1], s));
-        GMPM_TRY(launch_grid<R>(d_sc, bin, grid, d_cnt, cfg(), s));
+        GMPM_TRY(launch_grid<R>(d_sc, bin, grid, d_cnt, lc, s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[2], s));
         GMPM_TRY(launch_g2p<R>(d_sc, d_sc64, desc.precision == GMPM_PRECISION_FP32_FP64SVD ? d_sc64 : nullptr,
-                               st[cur], st[1 - cur], aux, bin, grid, d_cnt, cfg(), s));
+                               st[c], st[1 - c], aux, bin, grid, d_cnt, lc, s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[3], s));
-        launches += 4;  // p2g, grid, g2p, clock advance
-        cur = 1 - cur;
-        binned = false;
         return GMPM_OK;
     }
+
+    gmpm_status one_substep(cudaStream_t s, cudaEvent_t* ev) {
+        gmpm_status r = launch_one(s, cur, ev);
+        if (r != GMPM_OK) return r;
+        commit_substeps(1);
+        return GMPM_OK;
+    }
+
+    // batched stepping (SceneBase)
+    uint64_t uid() const override { return uid_; }
+    gmpm_context* context() const override { return ctx; }
+    int64_t particles() const override { return n; }
+    size_t device_bytes() const override { return dev_bytes_; }
+    int parity() const override { return cur; }
+    int kernels_per_substep() const override { return kBinningKernels + 4; }
+    gmpm_status launch_substep(cudaStream_t s, int c) override {
+        if (c != 0 && c != 1) return GMPM_INVALID_ARG;
+        return launch_one(s, c, nullptr);
+    }
+    void commit_substeps(int nsub) override {
+        launches += (int64_t)nsub * (kBinningKernels + 4);  // binning, p2g, grid, g2p, clock advance
+        if (nsub & 1) cur = 1 - cur;
+        binned = false;
+    }
+    void set_sm_share(int sms) override { share_ = sms > 0 ? sms : 0; }
+    int sm_share() const override { return share_; }
 
     gmpm_status substep(int nsteps, cudaStream_t s) override {
         if (nsteps < 0) return GMPM_INVALID_ARG;
@@ -688,10 +702,6 @@ void Scene<R>::mark_grid(cudaStream_t s) {
     launch_mark_grid(bin, s);
 }
 }  // namespace gmpm
-
-struct gmpm_scene {
-    gmpm::SceneBase* impl;
-};
 
 extern "C" {
 

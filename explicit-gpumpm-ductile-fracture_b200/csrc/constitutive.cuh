@@ -89,7 +89,11 @@ __device__ __forceinline__ void von_mises_update(const MaterialDev<MR>& m, R V0,
         }
         if (alpha > R(m.alpha_cap)) alpha_out = R(m.alpha_cap);
         const R tn = sqrt(tdev[0] * tdev[0] + tdev[1] * tdev[1] + tdev[2] * tdev[2]);
-        const R taudiv = (R(1) / tn) * p23 * g * tsum * dl;
+        // The reference divides by |tau_dev| (ExplicitTimeIntegrator.cu:242); its
+        // yield test uses the full trial stress, so a hydrostatic trial state
+        // (equal singular values, exact in FP32) can yield with tau_dev = 0.
+        // There is no deviator to scale then: the factor is 0 instead of NaN.
+        const R taudiv = tn > R(0) ? (R(1) / tn) * p23 * g * tsum * dl : R(0);
         const R p2 = (R(1) / R(3)) * tsum;
         R tnn[3];
 #pragma unroll

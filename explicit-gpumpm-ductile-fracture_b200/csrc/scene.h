@@ -1,0 +1,54 @@
+// Host-side scene interface shared by the C-ABI (api.cu), batched stepping
+// (batch.cu) and the serving loop (serve.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gmpm.h"
+
+struct gmpm_context {
+    int device;
+    int num_sms;
+    cudaDeviceProp prop;
+};
+
+namespace gmpm {
+
+gmpm_status cuda_status(cudaError_t e);
+
+// Common scene interface, implemented per precision (Scene<R> in api.cu).
+struct SceneBase {
+    virtual ~SceneBase() {}
+    virtual gmpm_status substep(int n, cudaStream_t s) = 0;
+    virtual gmpm_status substep_timed(int n, cudaStream_t s, gmpm_stage_times* out) = 0;
+    virtual gmpm_status rebin(cudaStream_t s) = 0;
+    virtual gmpm_status read_particles(int field, int dtype, int order, void* dst, size_t bytes, cudaStream_t s) = 0;
+    virtual gmpm_status read_binning(int array, void* dst, size_t bytes) = 0;
+    virtual gmpm_status diagnostics(gmpm_diag* out) = 0;
+    virtual gmpm_status sync() = 0;
+    virtual gmpm_status set_dt(double dt, cudaStream_t s) = 0;
+    virtual gmpm_status set_velocity_conditions(const gmpm_slab_bc* slabs, int ns, const gmpm_sphere_bc* spheres,
+                                                int nsp, cudaStream_t s) = 0;
+
+    // Batched stepping.  launch_substep issues one substep's kernels for the
+    // given state buffer without touching host bookkeeping, so it can be
+    // captured into a CUDA graph; commit_substeps records n substeps that
+    // were launched that way (buffer flips, launch counts).
+    virtual uint64_t uid() const = 0;
+    virtual gmpm_context* context() const = 0;
+    virtual int64_t particles() const = 0;
+    virtual size_t device_bytes() const = 0;
+    virtual int parity() const = 0;
+    virtual int kernels_per_substep() const = 0;
+    virtual gmpm_status launch_substep(cudaStream_t s, int parity) = 0;
+    virtual void commit_substeps(int n) = 0;
+    // Launch shapes are sized for this many SMs (0: the whole device).
+    virtual void set_sm_share(int sms) = 0;
+    virtual int sm_share() const = 0;
+};
+
+}  // namespace gmpm
+
+struct gmpm_scene {
+    gmpm::SceneBase* impl;
+};

@@ -101,6 +101,21 @@ class Geometry(C.Structure):
                 ("_pad0", C.c_int32), ("dx", C.c_double), ("origin", C.c_double * 3), ("seed", C.c_uint64)]
 
 
+class BatchOptions(C.Structure):
+    _fields_ = [("autotune", C.c_int32), ("trial_substeps", C.c_int32), ("streams", C.c_int32),
+                ("sm_share", C.c_int32)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("n_scenes", C.c_int32), ("streams", C.c_int32), ("tuned", C.c_int32), ("n_candidates", C.c_int32),
+                ("graph_nodes", C.c_int64), ("captures", C.c_int64), ("substeps", C.c_int64),
+                ("best_ms_per_substep", C.c_double), ("sm_share_small", C.c_int32),
+                ("sm_share_medium", C.c_int32), ("sm_share_large", C.c_int32), ("_pad0", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
+
+
 # Exported entry points and their argument types, exactly as declared in include/gmpm.h.
 SIGNATURES = {
     "gmpm_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -123,6 +138,12 @@ SIGNATURES = {
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
     "gmpm_generate_particles": (C.c_int, [C.POINTER(Geometry), C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                           C.POINTER(C.c_int32), C.c_int64]),
+    "gmpm_batch_options_defaults": (None, [C.POINTER(BatchOptions)]),
+    "gmpm_batch_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.POINTER(BatchOptions),
+                                    C.POINTER(C.c_void_p)]),
+    "gmpm_batch_substep": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "gmpm_batch_get_info": (C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
+    "gmpm_batch_destroy": (C.c_int, [C.c_void_p]),
 }
 
 _lib = None
@@ -291,3 +312,37 @@ class Scene:
         d = Diag()
         check(lib().gmpm_diagnostics(self.h, C.byref(d)), "diagnostics")
         return d.as_dict()
+
+
+class Batch:
+    """Independent scenes advanced together by one CUDA graph per substep (gmpm_batch)."""
+
+    def __init__(self, ctx: Context, scenes, autotune: bool = True, trial_substeps: int = 2, streams: int = 0,
+                 sm_share: int = 0):
+        self.ctx = ctx
+        self.scenes = list(scenes)  # keeps the scenes alive while the batch exists
+        opt = BatchOptions()
+        lib().gmpm_batch_options_defaults(C.byref(opt))
+        opt.autotune, opt.trial_substeps, opt.streams, opt.sm_share = int(autotune), trial_substeps, streams, sm_share
+        hs = (C.c_void_p * len(self.scenes))(*[sc.h for sc in self.scenes])
+        self.h = C.c_void_p()
+        check(lib().gmpm_batch_create(ctx.h, hs, len(self.scenes), C.byref(opt), C.byref(self.h)), "batch_create")
+
+    def substep(self, n: int = 1, stream: int | None = None) -> None:
+        check(lib().gmpm_batch_substep(self.h, int(n), C.c_void_p(stream) if stream else None), "batch_substep")
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        check(lib().gmpm_batch_get_info(self.h, C.byref(i)), "batch_get_info")
+        return i.as_dict()
+
+    def close(self) -> None:
+        if self.h:
+            lib().gmpm_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

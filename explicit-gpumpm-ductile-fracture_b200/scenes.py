@@ -10,6 +10,10 @@ parameters of the benchmark configurations:
   (33,554,432 particles), sphere impactor r=0.1 at 5 m/s, gravity -9.8.
 * ``plates_8m``    — the same scene at 8,388,608 particles: 4 plates of
   128x128x16 cells at dx=1/128 with 8 ppc.
+* ``notched_bar_batch`` — independent notched bars for batched stepping:
+  particle counts log-uniform in [10k, 500k], material parameters uniform
+  within +/-50% of the notched bar's, pull speed uniform in [0.2, 1.0] m/s,
+  FP32 with the FP64 SVD fallback.
 
 Material parameters follow the configurations: rho=1000, E=1e5 (per plate
 log-uniform in [5e4, 5e5] for the plate scenes), nu=0.3, yield 200 Pa with
@@ -81,6 +85,38 @@ def notched_bar(seed: int = 0, precision: int = G.PRECISION_FP32, cells=(16, 16,
     mass = np.full(len(pos), 1000.0 * d.particle_volume)
     vel = np.zeros_like(pos)
     return SceneSpec("notched_bar", d, pos, mass, vel, mat, substeps)
+
+
+def notched_bar_sized(n_target: int, seed: int = 0, precision: int = G.PRECISION_FP32_FP64SVD, E: float = 1e5,
+                      yield_stress: float = 200.0, density: float = 1000.0, pull: float = 0.5,
+                      dx: float = 1.0 / 128, ppc: int = 8, substeps: int = 1000) -> SceneSpec:
+    """Notched bar of a x a x 4a cells with about n_target particles; the grid
+    is sized to the bar (cubic, 8-cell margins)."""
+    a = max(4, int(round((n_target / (4.0 * ppc)) ** (1.0 / 3.0))))
+    res = max(32, -(-(4 * a + 16) // 4) * 4)
+    sp = notched_bar(seed=seed, precision=precision, cells=(a, a, 4 * a), ppc=ppc, dx=dx, pull=pull,
+                     notch=(1, max(1, a // 4)), res=res, substeps=substeps)
+    m = sp.desc.materials[0]
+    config_material(m, dx, E)
+    m.yield_stress = yield_stress
+    m.density = density
+    sp.masses = np.full(sp.n, density * sp.desc.particle_volume)
+    sp.name = f"notched_bar_{sp.n}"
+    return sp
+
+
+def notched_bar_batch(n_scenes: int = 64, seed: int = 0, lo: int = 10_000, hi: int = 500_000,
+                      precision: int = G.PRECISION_FP32_FP64SVD, substeps: int = 1000) -> list[SceneSpec]:
+    """Independent notched bars of uneven size and parameters (batched workload)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), n_scenes))
+    out = []
+    for k in range(n_scenes):
+        f = rng.uniform(0.5, 1.5, 3)
+        out.append(notched_bar_sized(int(sizes[k]), seed=seed * 1000 + k, precision=precision, E=1e5 * f[0],
+                                     yield_stress=200.0 * f[1], density=1000.0 * f[2],
+                                     pull=float(rng.uniform(0.2, 1.0)), substeps=substeps))
+    return out
 
 
 def _plate_scene(name: str, cells_xy: int, dx: float, ppc: int, margin: int, gap: int, res_y: int, seed: int,

@@ -361,6 +361,46 @@ typedef struct gmpm_scene_geometry {
 gmpm_status gmpm_generate_particles(const gmpm_scene_geometry* geom, int64_t* count,
                                     double* positions, int32_t* material_ids, int64_t capacity);
 
+/* ---- Batched stepping of independent scenes --------------------------------------------------
+ * No reference counterpart: the reference steps one scene per MPMSimulator::simulateStick call
+ * (Simulator.cpp:227-259).  A batch advances many independent scenes of uneven size, each with its
+ * own grid, with one CUDA graph launch per substep; every scene's binning, P2G, grid update and G2P
+ * is a parallel branch of that graph.  Each scene's results are the same as stepping it alone
+ * (bitwise in deterministic mode).  The autotuner times candidate launch shapes (the share of SMs
+ * each scene's kernels are sized for, per scene size class, and the number of concurrent branches)
+ * on the first substeps, which are real substeps, and keeps the fastest.
+ * Destroy a batch before any of its scenes; a scene may belong to several batches. */
+typedef struct gmpm_batch gmpm_batch;
+
+typedef struct gmpm_batch_options {
+    int32_t autotune;        /* 1: tune launch shapes on the first substeps (default 1) */
+    int32_t trial_substeps;  /* substeps per candidate, even and >= 2 (default 2) */
+    int32_t streams;         /* concurrent branches; 0: min(scenes, 32) */
+    int32_t sm_share;        /* SMs each scene's launch shapes are sized for when not tuning; 0: all */
+} gmpm_batch_options;
+
+typedef struct gmpm_batch_info {
+    int32_t n_scenes;
+    int32_t streams;          /* concurrent branches in use */
+    int32_t tuned;            /* 1 once tuning is finished (or disabled) */
+    int32_t n_candidates;     /* launch-shape candidates tried by the tuner */
+    int64_t graph_nodes;      /* nodes of one substep graph */
+    int64_t captures;         /* graphs captured so far */
+    int64_t substeps;         /* batched substeps launched */
+    double best_ms_per_substep; /* device time per substep of the chosen candidate (0 if untuned) */
+    int32_t sm_share_small;   /* chosen SM share for scenes below 50,000 particles (0: all SMs) */
+    int32_t sm_share_medium;  /* ... 50,000 to 200,000 particles */
+    int32_t sm_share_large;   /* ... 200,000 particles and above */
+    int32_t _pad0;
+} gmpm_batch_info;
+
+void gmpm_batch_options_defaults(gmpm_batch_options* opt);
+gmpm_status gmpm_batch_create(gmpm_context* ctx, gmpm_scene* const* scenes, int n_scenes,
+                              const gmpm_batch_options* opt /* NULL: defaults */, gmpm_batch** out);
+gmpm_status gmpm_batch_substep(gmpm_batch* batch, int n_substeps, void* stream);
+gmpm_status gmpm_batch_get_info(gmpm_batch* batch, gmpm_batch_info* out);
+gmpm_status gmpm_batch_destroy(gmpm_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

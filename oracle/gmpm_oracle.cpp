@@ -575,7 +575,11 @@ void von_mises(const MatConsts& mc, double V0, const double* Fin, double g, doub
         if (alpha > m->alpha_cap) alpha_out = m->alpha_cap;
         const double tn = std::sqrt(tau_dev_tr[0] * tau_dev_tr[0] + tau_dev_tr[1] * tau_dev_tr[1] +
                                     tau_dev_tr[2] * tau_dev_tr[2]);
-        const double taudiv = (1.0 / tn) * kP23 * g * tau_tr_sum * dlambda;
+        // ExplicitTimeIntegrator.cu:242 divides by |tau_dev|.  The yield test
+        // uses the full trial stress, so a purely hydrostatic trial state can
+        // yield with tau_dev = 0: there is no deviator to scale, and the factor
+        // is taken as 0 where the reference would produce 0 * inf = NaN.
+        const double taudiv = tn > 0.0 ? (1.0 / tn) * kP23 * g * tau_tr_sum * dlambda : 0.0;
         double tau_nn[3];
         const double p2 = (1.0 / 3.0) * tau_tr_sum;
         for (int k = 0; k < 3; ++k) tau_nn[k] = (tau_dev_tr[k] - tau_dev_tr[k] * taudiv) + p2;

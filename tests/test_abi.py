@@ -16,7 +16,7 @@ HEADER = ROOT / "include" / "gmpm.h"
 
 def declared_functions() -> list[str]:
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:gmpm_status|const char\*)\s+(gmpm_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:gmpm_status|const char\*|void)\s+(gmpm_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol(pkg):
@@ -37,7 +37,8 @@ def test_struct_layouts_match_header(pkg, tmp_path):
     G = pkg.gmpm
     structs = {"gmpm_material": G.Material, "gmpm_slab_bc": G.SlabBC, "gmpm_sphere_bc": G.SphereBC,
                "gmpm_scene_desc": G.SceneDesc, "gmpm_particle_init": G.ParticleInit, "gmpm_diag": G.Diag,
-               "gmpm_scene_geometry": G.Geometry, "gmpm_stage_times": G.StageTimes}
+               "gmpm_scene_geometry": G.Geometry, "gmpm_stage_times": G.StageTimes,
+               "gmpm_batch_options": G.BatchOptions, "gmpm_batch_info": G.BatchInfo}
     probe = tmp_path / "layout.c"
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gmpm.h"', "int main(void){"]
     for cname, ct in structs.items():
@@ -72,6 +73,17 @@ def test_null_arguments_are_rejected(pkg):
     assert L.gmpm_read_particles(None, 0, 0, 0, None, 0, None) == G.INVALID_ARG
     assert L.gmpm_diagnostics(None, None) == G.INVALID_ARG
     assert L.gmpm_scene_desc_reference_defaults(None, 1.0, 8, 8, 8) == G.INVALID_ARG
+    assert L.gmpm_batch_create(None, None, 0, None, None) == G.INVALID_ARG
+    assert L.gmpm_batch_substep(None, 1, None) == G.INVALID_ARG
+    assert L.gmpm_batch_get_info(None, None) == G.INVALID_ARG
+    assert L.gmpm_batch_destroy(None) == G.INVALID_ARG
+
+
+def test_batch_option_defaults(pkg):
+    G = pkg.gmpm
+    o = G.BatchOptions()
+    G.lib().gmpm_batch_options_defaults(C.byref(o))
+    assert (o.autotune, o.trial_substeps, o.streams, o.sm_share) == (1, 2, 0, 0)
 
 
 def test_reference_defaults(pkg):

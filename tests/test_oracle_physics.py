@@ -51,6 +51,21 @@ def test_constitutive_update_is_objective(oracle, material):
             assert np.isclose(a[k], b[k], rtol=1e-9, atol=1e-18), k
 
 
+def test_hydrostatic_trial_state_stays_finite(oracle, pkg):
+    """A purely hydrostatic stretch of a damaged particle passes the
+    reference's yield test (it uses the full trial-stress norm) with a zero
+    deviator; the projection must not divide 0 by 0.  State taken from a grip
+    particle of a batched notched bar that went non-finite in FP32."""
+    d = pkg.gmpm.reference_defaults(1.0 / 128, (76, 76, 76))
+    pkg.scenes.config_material(d.materials[0], 1.0 / 128, 61493.26)
+    m = d.materials[0]
+    m.yield_stress = 245.8
+    r = vm(oracle, m, 1e-6 / 8, 1.0038 * np.eye(3), g=0.328, alpha=0.5087, c=0.5247, psi=4.1432)
+    for k in ("F", "sigma"):
+        assert np.all(np.isfinite(r[k])), k
+    assert np.isfinite(r["vol"]) and r["alpha"] > 0.5087  # the plastic branch was taken
+
+
 def test_plastic_update_respects_caps(oracle, material):
     F = np.diag([1.5, 0.8, 0.9])
     r = vm(oracle, material, 1e-6, F)
