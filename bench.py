@@ -352,6 +352,24 @@ def run_batched(pkg, local_rank: int, steps: int, plain_steps: int, n_scenes: in
                          "FP32 + FP64 SVD fallback, dx=1/128, 8 ppc")
 
 
+def run_served(pkg, local_rank: int, duration_s: float) -> dict:
+    """The served workload: Poisson arrivals (20/s) of notched-bar and
+    plate-impact solves (50/50; 20k-2M particles log-uniform; horizons
+    200-2000 substeps), admitted against a 120 GB budget into one continuous
+    batch.  Latency = finish - submit of each completed request."""
+    import torch
+
+    G = pkg.gmpm
+    torch.cuda.set_device(local_rank)
+    ctx = G.Context(local_rank)
+    stream = torch.cuda.Stream(torch.device("cuda", local_rank))
+    from gmpm_b200 import serving  # noqa: E402  (package loaded by load_package)
+    r = serving.run_served(ctx, duration_s=duration_s, rate_hz=20.0, seed=0, stream=stream.cuda_stream)
+    r["workload"] = ("Poisson 20 req/s, notched bar or plate impact 50/50, 20k-2M particles log-uniform, "
+                     "horizons U[200,2000] substeps, params +/-50%, 120 GB budget, FP32 + FP64 SVD fallback")
+    return r
+
+
 def sizeof_velocity_conditions(dt) -> int:
     # int n_slabs, n_spheres, slab_axis[4]; Real lo[4], hi[4], vel[4][3], c[2][3], r[2], v[2][3]
     r = np.dtype(dt).itemsize
@@ -367,9 +385,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="plates_33m",
-                    choices=["plates_33m", "plates_8m", "notched_bar", "batched64"])
+                    choices=["plates_33m", "plates_8m", "notched_bar", "batched64", "served"])
+    ap.add_argument("--duration", type=float, default=600.0, help="served workload: seconds of arrivals")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload object of the line")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-workload object of the line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -413,6 +433,18 @@ def main():
         print(json.dumps(line))
         return
 
+    if args.workload == "served":
+        if rank != 0:
+            return
+        r = run_served(pkg, local_rank, args.duration)
+        line = dict(metric="particle-substeps/sec", value=r["particle_substeps_per_s"], unit="particle-substeps/s",
+                    n_gpus=1, steps=r["substeps"], warmup=0, ms_per_step=None, higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+                    config=dict(workload=r["workload"], parallelism="continuous batching"),
+                    p50_latency_s=r["p50_latency_s"], p99_latency_s=r["p99_latency_s"], served=r)
+        print(json.dumps(line))
+        return
+
     dist = None
     if world > 1:
         import datetime
@@ -438,6 +470,9 @@ def main():
                                      "plain_sequential", "speedup_vs_plain", "gpu_launches", "status", "workload")}
         batched["autotune"] = {k: b["autotune"][k] for k in ("streams", "n_candidates", "sm_share_small",
                                                               "sm_share_medium", "sm_share_large", "graph_nodes")}
+    served = None
+    if rank == 0 and world == 1 and not args.no_served:
+        served = run_served(pkg, local_rank, duration_s=20.0)
     if rank == 0:
         sp = res["sp"]
         k = res["kernels"][res["dom"]]
@@ -453,7 +488,7 @@ def main():
                           peak_source=res["peaks"]["source"]),
             kernels=res["kernels"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
             gpu_launches=res["launches"], status=pkg.gmpm.STATUS_NAMES.get(res["status"], res["status"]),
-            n_blocks=res["diag"]["n_blocks"], n_grid_blocks=res["diag"]["n_grid_blocks"], batched=batched)
+            n_blocks=res["diag"]["n_blocks"], n_grid_blocks=res["diag"]["n_grid_blocks"], batched=batched, served=served)
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

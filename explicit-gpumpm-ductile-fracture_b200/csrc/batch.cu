@@ -15,6 +15,7 @@
 // branches, on the first substeps (real substeps: results do not depend on
 // launch shapes) and keeps the fastest.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -62,6 +63,7 @@ struct Batch {
     double best_ms = 0;
     Candidate best{};
     int64_t captures = 0, substeps = 0, graph_nodes = 0;
+    double capture_s = 0;
 
     ~Batch() { release(); }
 
@@ -145,6 +147,13 @@ struct Batch {
     }
 
     gmpm_status capture(int k, cudaGraphExec_t* out) {
+        const auto tc = std::chrono::steady_clock::now();
+        gmpm_status r = capture_graph(k, out);
+        capture_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - tc).count();
+        return r;
+    }
+
+    gmpm_status capture_graph(int k, cudaGraphExec_t* out) {
         BATCH_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
         gmpm_status r = GMPM_OK;
         cudaError_t e = cudaEventRecord(fork, cap);
@@ -263,6 +272,7 @@ struct Batch {
         o->sm_share_small = current.share[0];
         o->sm_share_medium = current.share[1];
         o->sm_share_large = current.share[2];
+        o->capture_seconds = capture_s;
     }
 };
 

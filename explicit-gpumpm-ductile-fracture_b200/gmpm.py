@@ -110,10 +110,36 @@ class BatchInfo(C.Structure):
     _fields_ = [("n_scenes", C.c_int32), ("streams", C.c_int32), ("tuned", C.c_int32), ("n_candidates", C.c_int32),
                 ("graph_nodes", C.c_int64), ("captures", C.c_int64), ("substeps", C.c_int64),
                 ("best_ms_per_substep", C.c_double), ("sm_share_small", C.c_int32),
-                ("sm_share_medium", C.c_int32), ("sm_share_large", C.c_int32), ("_pad0", C.c_int32)]
+                ("sm_share_medium", C.c_int32), ("sm_share_large", C.c_int32), ("_pad0", C.c_int32),
+                ("capture_seconds", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_live", C.c_int32), ("autotune", C.c_int32)]
+
+
+class RequestStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("n_particles", C.c_int64),
+                ("substeps_done", C.c_int64), ("horizon", C.c_int64), ("submit_time", C.c_double),
+                ("admit_time", C.c_double), ("finish_time", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "admitted", "completed", "failed", "live", "queued",
+                                          "substeps", "particle_substeps", "batches", "device_bytes_in_use",
+                                          "capture_microseconds")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+REQUEST_QUEUED, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3
 
 
 # Exported entry points and their argument types, exactly as declared in include/gmpm.h.
@@ -144,6 +170,16 @@ SIGNATURES = {
     "gmpm_batch_substep": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "gmpm_batch_get_info": (C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
     "gmpm_batch_destroy": (C.c_int, [C.c_void_p]),
+    "gmpm_server_options_defaults": (None, [C.POINTER(ServerOptions)]),
+    "gmpm_server_create": (C.c_int, [C.c_void_p, C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    "gmpm_server_submit": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(ParticleInit), C.c_int64,
+                                     C.POINTER(C.c_int64)]),
+    "gmpm_server_step": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "gmpm_server_poll": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(RequestStatus)]),
+    "gmpm_server_read": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_size_t]),
+    "gmpm_server_release": (C.c_int, [C.c_void_p, C.c_int64]),
+    "gmpm_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "gmpm_server_destroy": (C.c_int, [C.c_void_p]),
 }
 
 _lib = None
@@ -339,6 +375,73 @@ class Batch:
     def close(self) -> None:
         if self.h:
             lib().gmpm_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching serving loop (gmpm_server)."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int | None = None, max_live: int | None = None,
+                 autotune: bool = True):
+        self.ctx = ctx
+        opt = ServerOptions()
+        lib().gmpm_server_options_defaults(C.byref(opt))
+        if hbm_budget_bytes is not None:
+            opt.hbm_budget_bytes = int(hbm_budget_bytes)
+        if max_live is not None:
+            opt.max_live = int(max_live)
+        opt.autotune = int(autotune)
+        self.h = C.c_void_p()
+        check(lib().gmpm_server_create(ctx.h, C.byref(opt), C.byref(self.h)), "server_create")
+
+    def submit(self, desc: SceneDesc, positions: np.ndarray, masses: np.ndarray, velocities=None,
+               material_ids=None, horizon: int = 1) -> int:
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        m = np.ascontiguousarray(masses, dtype=np.float64).reshape(-1)
+        v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float64).reshape(-1, 3)
+        mid = None if material_ids is None else np.ascontiguousarray(material_ids, dtype=np.int32).reshape(-1)
+        init = ParticleInit(len(pos), _dptr(pos), _dptr(v), _dptr(m), _iptr(mid))
+        rid = C.c_int64()
+        check(lib().gmpm_server_submit(self.h, C.byref(desc), C.byref(init), int(horizon), C.byref(rid)),
+              "server_submit")
+        return rid.value
+
+    def submit_spec(self, spec, horizon: int) -> int:
+        return self.submit(spec.desc, spec.positions, spec.masses, spec.velocities, spec.material_ids, horizon)
+
+    def step(self, n: int = 1, stream: int | None = None) -> None:
+        check(lib().gmpm_server_step(self.h, int(n), C.c_void_p(stream) if stream else None), "server_step")
+
+    def poll(self, rid: int) -> dict:
+        st = RequestStatus()
+        check(lib().gmpm_server_poll(self.h, int(rid), C.byref(st)), "server_poll")
+        return st.as_dict()
+
+    def read(self, rid: int, field: str) -> np.ndarray:
+        st = self.poll(rid)
+        nc = FIELD_COMPONENTS[field]
+        out = np.empty((st["n_particles"], nc), dtype=np.float32)
+        check(lib().gmpm_server_read(self.h, int(rid), FIELD[field], out.ctypes.data_as(C.c_void_p), out.nbytes),
+              f"server_read({field})")
+        return out if nc > 1 else out.reshape(-1)
+
+    def release(self, rid: int) -> None:
+        check(lib().gmpm_server_release(self.h, int(rid)), "server_release")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib().gmpm_server_get_stats(self.h, C.byref(st)), "server_get_stats")
+        return st.as_dict()
+
+    def close(self) -> None:
+        if self.h:
+            lib().gmpm_server_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

@@ -170,6 +170,36 @@ def plates_small(cells_xy: int = 32, seed: int = 0, precision: int = G.PRECISION
     return _plate_scene(f"plates_{cells_xy}", cells_xy, dx, 8, 8, 4, 96, seed, precision, substeps)
 
 
+def plates_sized(n_target: int, seed: int = 0, precision: int = G.PRECISION_FP32_FP64SVD, e_scale: float = 1.0,
+                 substeps: int = 1000) -> SceneSpec:
+    """Plate-impact scene (4 plates of c x c x 16 cells at dx=1/128, 8 ppc) with
+    about n_target particles; the sphere radius is capped at 0.4 plate widths."""
+    dx = 1.0 / 128
+    c = max(4, int(round((n_target / (4 * 16 * 8)) ** 0.5)))
+    sp = _plate_scene(f"plates_{c}", c, dx, 8, 8, 4, 96, seed, precision, substeps)
+    sp.desc.spheres[0].radius = min(0.1, 0.4 * c * dx)
+    top = 8 * dx + (4 * 16 + 3 * 4) * dx
+    sp.desc.spheres[0].center[1] = top + sp.desc.spheres[0].radius + 2 * dx
+    for k in range(sp.desc.n_materials):
+        config_material(sp.desc.materials[k], dx, sp.desc.materials[k].youngs_modulus * e_scale)
+    return sp
+
+
+def served_request(rng: np.random.Generator, k: int, lo: int = 20_000, hi: int = 2_000_000) -> tuple[SceneSpec, int]:
+    """One request of the served workload: a notched bar or a plate impact
+    (50/50), size log-uniform in [lo, hi], horizon uniform in [200, 2000]
+    substeps, parameters within +/-50% of the notched bar's."""
+    n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+    horizon = int(rng.integers(200, 2001))
+    f = rng.uniform(0.5, 1.5, 3)
+    if rng.random() < 0.5:
+        sp = notched_bar_sized(n, seed=k, E=1e5 * f[0], yield_stress=200.0 * f[1], density=1000.0 * f[2],
+                               pull=float(rng.uniform(0.2, 1.0)), substeps=horizon)
+    else:
+        sp = plates_sized(n, seed=k, e_scale=float(f[0]), substeps=horizon)
+    return sp, horizon
+
+
 def blob(n_side: int = 12, ppc: int = 8, seed: int = 3, precision: int = G.PRECISION_FP32, dx: float = 1.0 / 64,
          res: int = 64, velocity=(0.3, -0.2, 0.1), spin: float = 2.0) -> SceneSpec:
     """Free-flying box with translation + rotation, no gravity, no walls or

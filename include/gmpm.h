@@ -392,6 +392,7 @@ typedef struct gmpm_batch_info {
     int32_t sm_share_medium;  /* ... 50,000 to 200,000 particles */
     int32_t sm_share_large;   /* ... 200,000 particles and above */
     int32_t _pad0;
+    double capture_seconds;   /* host time spent capturing and instantiating graphs */
 } gmpm_batch_info;
 
 void gmpm_batch_options_defaults(gmpm_batch_options* opt);
@@ -400,6 +401,67 @@ gmpm_status gmpm_batch_create(gmpm_context* ctx, gmpm_scene* const* scenes, int 
 gmpm_status gmpm_batch_substep(gmpm_batch* batch, int n_substeps, void* stream);
 gmpm_status gmpm_batch_get_info(gmpm_batch* batch, gmpm_batch_info* out);
 gmpm_status gmpm_batch_destroy(gmpm_batch* batch);
+
+/* ---- Serving loop (continuous batching) --------------------------------------------------------
+ * No reference counterpart (the reference runs one scene per process from its GLUT loop,
+ * gl_main.cpp:304-314).  Requests queue on submit.  Each gmpm_server_step admits queued requests in
+ * arrival order while the device-memory budget allows, advances every live scene together through
+ * one batch (a CUDA graph launch per substep), never past a request's horizon, and retires requests
+ * that reached it: their final position, velocity, F and damage are copied to host memory (FP32,
+ * original particle order) and the scene's device memory is freed for waiting requests.  A result
+ * does not depend on which requests shared the GPU (bitwise in deterministic mode).  One host
+ * thread drives a server. */
+typedef struct gmpm_server gmpm_server;
+
+typedef enum gmpm_request_state {
+    GMPM_REQUEST_QUEUED = 0,
+    GMPM_REQUEST_RUNNING = 1,
+    GMPM_REQUEST_DONE = 2,
+    GMPM_REQUEST_FAILED = 3
+} gmpm_request_state;
+
+typedef struct gmpm_server_options {
+    int64_t hbm_budget_bytes;   /* device memory admitted scenes may hold; 0: unlimited (default 120 GB) */
+    int32_t max_live;           /* scenes advanced together (default 64; 0: unlimited).  Every change of
+                                   the live set re-captures the batch graph, whose size grows with it */
+    int32_t autotune;           /* tune the first batch's launch shapes and reuse them (default 1) */
+} gmpm_server_options;
+
+typedef struct gmpm_request_status {
+    int32_t state;              /* gmpm_request_state */
+    int32_t status;             /* gmpm_status of the scene (creation, flags at retirement) */
+    int64_t n_particles;
+    int64_t substeps_done;
+    int64_t horizon;
+    double submit_time;         /* seconds since the server was created */
+    double admit_time;
+    double finish_time;
+} gmpm_request_status;
+
+typedef struct gmpm_server_stats {
+    int64_t submitted, admitted, completed, failed;
+    int64_t live, queued;
+    int64_t substeps;           /* batched substeps run */
+    int64_t particle_substeps;  /* sum over live scenes of particles x substeps */
+    int64_t batches;            /* batches built (one per change of the live set) */
+    int64_t device_bytes_in_use;
+    int64_t capture_microseconds; /* host time spent capturing batch graphs */
+} gmpm_server_stats;
+
+void gmpm_server_options_defaults(gmpm_server_options* opt);
+gmpm_status gmpm_server_create(gmpm_context* ctx, const gmpm_server_options* opt /* NULL: defaults */,
+                               gmpm_server** out);
+/* Copies the particle arrays; the scene is created on admission. */
+gmpm_status gmpm_server_submit(gmpm_server* srv, const gmpm_scene_desc* desc, const gmpm_particle_init* init,
+                               int64_t horizon_substeps, int64_t* request_id);
+gmpm_status gmpm_server_step(gmpm_server* srv, int n_substeps, void* stream);
+gmpm_status gmpm_server_poll(gmpm_server* srv, int64_t request_id, gmpm_request_status* out);
+/* Final field of a finished request: GMPM_FIELD_POSITION, _VELOCITY, _F or _DAMAGE, FP32. */
+gmpm_status gmpm_server_read(gmpm_server* srv, int64_t request_id, int field, float* dst, size_t bytes);
+/* Forget a finished or failed request (frees its host results). */
+gmpm_status gmpm_server_release(gmpm_server* srv, int64_t request_id);
+gmpm_status gmpm_server_get_stats(gmpm_server* srv, gmpm_server_stats* out);
+gmpm_status gmpm_server_destroy(gmpm_server* srv);
 
 #ifdef __cplusplus
 }

@@ -38,7 +38,9 @@ def test_struct_layouts_match_header(pkg, tmp_path):
     structs = {"gmpm_material": G.Material, "gmpm_slab_bc": G.SlabBC, "gmpm_sphere_bc": G.SphereBC,
                "gmpm_scene_desc": G.SceneDesc, "gmpm_particle_init": G.ParticleInit, "gmpm_diag": G.Diag,
                "gmpm_scene_geometry": G.Geometry, "gmpm_stage_times": G.StageTimes,
-               "gmpm_batch_options": G.BatchOptions, "gmpm_batch_info": G.BatchInfo}
+               "gmpm_batch_options": G.BatchOptions, "gmpm_batch_info": G.BatchInfo,
+               "gmpm_server_options": G.ServerOptions, "gmpm_request_status": G.RequestStatus,
+               "gmpm_server_stats": G.ServerStats}
     probe = tmp_path / "layout.c"
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gmpm.h"', "int main(void){"]
     for cname, ct in structs.items():
@@ -77,6 +79,10 @@ def test_null_arguments_are_rejected(pkg):
     assert L.gmpm_batch_substep(None, 1, None) == G.INVALID_ARG
     assert L.gmpm_batch_get_info(None, None) == G.INVALID_ARG
     assert L.gmpm_batch_destroy(None) == G.INVALID_ARG
+    assert L.gmpm_server_create(None, None, None) == G.INVALID_ARG
+    assert L.gmpm_server_step(None, 1, None) == G.INVALID_ARG
+    assert L.gmpm_server_poll(None, 1, None) == G.INVALID_ARG
+    assert L.gmpm_server_destroy(None) == G.INVALID_ARG
 
 
 def test_batch_option_defaults(pkg):
