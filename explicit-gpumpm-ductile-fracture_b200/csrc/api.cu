@@ -25,6 +25,22 @@ gmpm_status cuda_status(cudaError_t e) {
 
 std::atomic<uint64_t> g_scene_uid{1};
 
+// Checkpoint file: this header, the scene description, then every particle
+// plane of the state (n values each, in the internal order).
+constexpr char kSnapshotMagic[8] = {'G', 'M', 'P', 'M', 'S', 'N', 'A', 'P'};
+constexpr uint32_t kSnapshotVersion = 1;
+struct SnapshotHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t real_bytes;
+    uint32_t desc_bytes;
+    uint32_t _pad;
+    int64_t n;
+    double time;
+    int64_t substeps;
+    double dt;
+};
+
 namespace {
 
 #define GMPM_TRY(expr)                                   \
@@ -151,6 +167,23 @@ void fill_scene_dev(const gmpm_scene_desc& d, int key_bits, SceneDev<R>& s) {
     s.svd_fallback_ratio = (R)d.svd_fallback_ratio;
     s.dx_d = d.dx;
     s.inv_dx_d = 1.0 / d.dx;
+    s.adaptive_dt = d.adaptive_dt;
+    s.dt_max = d.dt;
+    s.cfl_dx = d.dx * (d.cfl_number > 0 ? d.cfl_number : (double)0.3f);
+}
+
+// First substep's dt in adaptive mode: the CFL bound of the initial velocities
+// (MPMSimulator::computeDt, Simulator.cpp:200-225).
+double initial_cfl_dt(const gmpm_scene_desc& d, const gmpm_particle_init& init) {
+    double v2max = 0.0;
+    if (init.velocities)
+        for (int64_t p = 0; p < init.count; ++p) {
+            const double* v = init.velocities + 3 * p;
+            v2max = std::max(v2max, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        }
+    const double vmax = std::sqrt(v2max);
+    const double cdx = d.dx * (d.cfl_number > 0 ? d.cfl_number : (double)0.3f);
+    return (vmax > 0 && cdx / vmax < d.dt) ? cdx / vmax : d.dt;
 }
 
 gmpm_status validate(const gmpm_scene_desc* d, const gmpm_particle_init* init) {
@@ -174,6 +207,7 @@ gmpm_status validate(const gmpm_scene_desc* d, const gmpm_particle_init* init) {
     if (d->precision < 0 || d->precision > 2) return GMPM_INVALID_ARG;
     if (d->phase_field < 0 || d->phase_field > 1) return GMPM_INVALID_ARG;
     if (d->block_capacity < 0) return GMPM_INVALID_ARG;
+    if (d->adaptive_dt < 0 || d->adaptive_dt > 1 || !(d->cfl_number >= 0)) return GMPM_INVALID_ARG;
     if (init->material_ids)
         for (int64_t p = 0; p < init->count; ++p)
             if (init->material_ids[p] < 0 || init->material_ids[p] >= d->n_materials) return GMPM_INVALID_ARG;
@@ -266,6 +300,11 @@ struct Scene : SceneBase {
         fill_scene_dev<R>(desc, key_bits, h);
         SceneDev<double> h64{};
         fill_scene_dev<double>(desc, key_bits, h64);
+        if (desc.adaptive_dt) {
+            const double dt0 = initial_cfl_dt(desc, *init);
+            h.dt = (R)dt0;
+            h64.dt = dt0;
+        }
         GMPM_TRY(alloc(&d_sc, 1));
         GMPM_TRY(alloc(&d_sc64, 1));
         GMPM_TRY(cudaMemcpy(d_sc, &h, sizeof(h), cudaMemcpyHostToDevice));
@@ -462,6 +501,76 @@ struct Scene : SceneBase {
     void set_sm_share(int sms) override { share_ = sms > 0 ? sms : 0; }
     int sm_share() const override { return share_; }
 
+    // ---- checkpoint ---------------------------------------------------------
+    // Every particle plane of the current state, in the internal order, with
+    // the clock; binning and grid are rebuilt by the next substep.
+    template <typename F>
+    void for_each_plane(int c, F&& f) {
+        for (int a = 0; a < 3; ++a) f(st[c].x[a], sizeof(R));
+        for (int q = 0; q < 9; ++q) f(st[c].F[q], sizeof(R));
+        f(st[c].c, sizeof(R));
+        f(st[c].alpha, sizeof(R));
+        f(st[c].psi, sizeof(R));
+        f(st[c].m, sizeof(R));
+        f(st[c].id, sizeof(uint32_t));
+        for (int a = 0; a < 3; ++a) f(aux.v[a], sizeof(R));
+        for (int q = 0; q < 9; ++q) f(aux.B[q], sizeof(R));
+        for (int q = 0; q < 6; ++q) f(aux.sigma[q], sizeof(R));
+        f(aux.vol, sizeof(R));
+        f(aux.FP, sizeof(R));
+        for (int a = 0; a < 3; ++a) f(aux.q[a], sizeof(R));
+    }
+
+    gmpm_status save(const char* path) override {
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        GMPM_TRY(cudaDeviceSynchronize());
+        SnapshotHeader h{};
+        std::memcpy(h.magic, kSnapshotMagic, sizeof(h.magic));
+        h.version = kSnapshotVersion;
+        h.real_bytes = (uint32_t)sizeof(R);
+        h.desc_bytes = (uint32_t)sizeof(gmpm_scene_desc);
+        h.n = n;
+        Counters c{};
+        GMPM_TRY(cudaMemcpy(&c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost));
+        GMPM_TRY(cudaMemcpy(&h.dt, &d_sc64->dt, sizeof(double), cudaMemcpyDeviceToHost));
+        h.time = c.time;
+        h.substeps = c.substeps;
+        FILE* f = std::fopen(path, "wb");
+        if (!f) return GMPM_IO_ERROR;
+        bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 && std::fwrite(&desc, sizeof(desc), 1, f) == 1;
+        std::vector<unsigned char> buf((size_t)n * sizeof(double));
+        for_each_plane(cur, [&](const void* p, size_t esz) {
+            if (!ok) return;
+            ok = cudaMemcpy(buf.data(), p, (size_t)n * esz, cudaMemcpyDeviceToHost) == cudaSuccess &&
+                 std::fwrite(buf.data(), esz, (size_t)n, f) == (size_t)n;
+        });
+        ok = (std::fclose(f) == 0) && ok;
+        return ok ? GMPM_OK : GMPM_IO_ERROR;
+    }
+
+    // Overwrite the freshly created state with a snapshot's planes and clock.
+    gmpm_status restore(FILE* f, const SnapshotHeader& h) {
+        std::vector<unsigned char> buf((size_t)n * sizeof(double));
+        bool ok = true;
+        for_each_plane(cur, [&](void* p, size_t esz) {
+            if (!ok) return;
+            ok = std::fread(buf.data(), esz, (size_t)n, f) == (size_t)n &&
+                 cudaMemcpy(p, buf.data(), (size_t)n * esz, cudaMemcpyHostToDevice) == cudaSuccess;
+        });
+        if (!ok) return GMPM_IO_ERROR;
+        Counters c{};
+        GMPM_TRY(cudaMemcpy(&c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost));
+        c.time = h.time;
+        c.substeps = h.substeps;
+        GMPM_TRY(cudaMemcpy(d_cnt, &c, sizeof(c), cudaMemcpyHostToDevice));
+        const R dtr = (R)h.dt;
+        GMPM_TRY(cudaMemcpy(&d_sc->dt, &dtr, sizeof(R), cudaMemcpyHostToDevice));
+        GMPM_TRY(cudaMemcpy(&d_sc64->dt, &h.dt, sizeof(double), cudaMemcpyHostToDevice));
+        GMPM_TRY(cudaDeviceSynchronize());
+        binned = false;
+        return GMPM_OK;
+    }
+
     gmpm_status substep(int nsteps, cudaStream_t s) override {
         if (nsteps < 0) return GMPM_INVALID_ARG;
         GMPM_TRY(cudaSetDevice(ctx->device));
@@ -608,6 +717,7 @@ struct Scene : SceneBase {
         out->n_grid_blocks = h.n_grid_blocks;
         out->flags = h.flags;
         out->kernel_launches = launches;
+        GMPM_TRY(cudaMemcpy(&out->dt, &d_sc64->dt, sizeof(double), cudaMemcpyDeviceToHost));
         return GMPM_OK;
     }
 
@@ -631,6 +741,9 @@ struct Scene : SceneBase {
         dt_staging[k].d = dt;
         GMPM_TRY(cudaMemcpyAsync(&d_sc->dt, &dt_staging[k].r, sizeof(R), cudaMemcpyHostToDevice, s));
         GMPM_TRY(cudaMemcpyAsync(&d_sc64->dt, &dt_staging[k].d, sizeof(double), cudaMemcpyHostToDevice, s));
+        // in adaptive mode dt is the upper bound of the CFL step
+        GMPM_TRY(cudaMemcpyAsync(&d_sc->dt_max, &dt_staging[k].d, sizeof(double), cudaMemcpyHostToDevice, s));
+        GMPM_TRY(cudaMemcpyAsync(&d_sc64->dt_max, &dt_staging[k].d, sizeof(double), cudaMemcpyHostToDevice, s));
         GMPM_TRY(cudaEventRecord(dt_done[k], s));
         desc.dt = dt;
         return GMPM_OK;
@@ -716,6 +829,7 @@ const char* gmpm_status_string(gmpm_status s) {
         case GMPM_CUDA_ERROR: return "CUDA error";
         case GMPM_NOT_SUPPORTED: return "not supported";
         case GMPM_NO_DEVICE: return "no CUDA device";
+        case GMPM_IO_ERROR: return "checkpoint file error";
         default: return "unknown status";
     }
 }
@@ -782,6 +896,8 @@ gmpm_status gmpm_scene_desc_reference_defaults(gmpm_scene_desc* d, double dx, in
     d->phase_field = GMPM_PHASE_FIELD_EXPLICIT;
     d->deterministic = 1;
     d->svd_fallback_ratio = 1e-3;
+    d->adaptive_dt = 0;
+    d->cfl_number = (double)0.3f;                  // Simulator.cpp:211
     return GMPM_OK;
 }
 
@@ -810,6 +926,71 @@ gmpm_status gmpm_scene_create(gmpm_context* ctx, const gmpm_scene_desc* desc, co
         return r;
     }
     *out = s;
+    return GMPM_OK;
+}
+
+gmpm_status gmpm_scene_save(gmpm_scene* s, const char* path) {
+    if (!s || !path) return GMPM_INVALID_ARG;
+    return s->impl->save(path);
+}
+
+gmpm_status gmpm_scene_load(gmpm_context* ctx, const char* path, gmpm_scene** out) {
+    using namespace gmpm;
+    if (!ctx || !path || !out) return GMPM_INVALID_ARG;
+    *out = nullptr;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return GMPM_IO_ERROR;
+    struct Closer {
+        FILE* f;
+        ~Closer() { std::fclose(f); }
+    } closer{f};
+    SnapshotHeader h{};
+    gmpm_scene_desc desc{};
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, kSnapshotMagic, 8) != 0 ||
+        h.version != kSnapshotVersion || h.desc_bytes != sizeof(gmpm_scene_desc) || h.n <= 0 ||
+        std::fread(&desc, sizeof(desc), 1, f) != 1)
+        return GMPM_IO_ERROR;
+    const size_t rb = desc.precision == GMPM_PRECISION_FP64 ? 8 : 4;
+    if (h.real_bytes != rb) return GMPM_IO_ERROR;
+    const long base = std::ftell(f);
+    const int64_t n = h.n;
+    // positions (planes 0-2), mass (plane 15) and ids (plane 16) build the scene;
+    // then every plane is restored over it
+    std::vector<double> pos((size_t)n * 3), mass((size_t)n);
+    std::vector<int32_t> mat((size_t)n);
+    {
+        std::vector<unsigned char> buf((size_t)n * rb);
+        auto read_plane = [&](int64_t plane_index, std::vector<double>& dst, int stride, int comp) -> bool {
+            if (std::fseek(f, base + (long)(plane_index * n * (int64_t)rb), SEEK_SET) != 0) return false;
+            if (std::fread(buf.data(), rb, (size_t)n, f) != (size_t)n) return false;
+            for (int64_t p = 0; p < n; ++p)
+                dst[(size_t)(p * stride + comp)] =
+                    rb == 8 ? reinterpret_cast<const double*>(buf.data())[p] : reinterpret_cast<const float*>(buf.data())[p];
+            return true;
+        };
+        for (int a = 0; a < 3; ++a)
+            if (!read_plane(a, pos, 3, a)) return GMPM_IO_ERROR;
+        if (!read_plane(15, mass, 1, 0)) return GMPM_IO_ERROR;
+        std::vector<uint32_t> ids((size_t)n);
+        if (std::fseek(f, base + (long)(16 * n * (int64_t)rb), SEEK_SET) != 0 ||
+            std::fread(ids.data(), 4, (size_t)n, f) != (size_t)n)
+            return GMPM_IO_ERROR;
+        for (int64_t p = 0; p < n; ++p) mat[(size_t)p] = (int32_t)(ids[(size_t)p] >> 28);
+    }
+    gmpm_particle_init init{n, pos.data(), nullptr, mass.data(), mat.data()};
+    gmpm_scene* sc = nullptr;
+    gmpm_status r = gmpm_scene_create(ctx, &desc, &init, &sc);
+    if (r != GMPM_OK) return r;
+    std::fseek(f, base, SEEK_SET);
+    if (desc.precision == GMPM_PRECISION_FP64)
+        r = static_cast<Scene<double>*>(sc->impl)->restore(f, h);
+    else
+        r = static_cast<Scene<float>*>(sc->impl)->restore(f, h);
+    if (r != GMPM_OK) {
+        gmpm_scene_destroy(sc);
+        return r;
+    }
+    *out = sc;
     return GMPM_OK;
 }
 

@@ -71,6 +71,9 @@ struct SceneDev {
     Real svd_fallback_ratio;
     Real mobility;          // scene mobility used by the grid phase-field update (material 0)
     double dx_d, inv_dx_d;  // binning arithmetic is always FP64
+    int adaptive_dt;        // CFL time step from the previous G2P's max speed
+    double dt_max;          // the scene's dt: upper bound of the adaptive step
+    double cfl_dx;          // cfl_number * dx
 };
 
 // Counters and flags living in device memory (written by kernels, read by host on demand).
@@ -81,6 +84,7 @@ struct Counters {
     int pad;
     double time;
     long long substeps;
+    unsigned long long vmax2_bits;  // max |v_p|^2 of the last G2P (FP64 bits; non-negative, so integer order)
 };
 
 // ---- SPGrid page keys -----------------------------------------------------

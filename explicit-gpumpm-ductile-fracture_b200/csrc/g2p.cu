@@ -162,6 +162,7 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
     const bool fallback = sc->fp64_svd_fallback && sc64 != nullptr;
     const R ratio = sc->svd_fallback_ratio;
     unsigned int flags = 0;
+    double v2max = 0.0;  // max |v_p|^2 of this thread's particles (adaptive dt)
 
     // prologue: meta of units 0 and 1, data of unit 0
     UnitIter it;
@@ -275,6 +276,7 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
             }
 #pragma unroll
             for (int q = 0; q < 9; ++q) aux.B[q][slot] = Bn[q];
+            if (sc->adaptive_dt) v2max = fmax(v2max, (double)(vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]));
             out.c[slot] = c_new;
             out.m[slot] = S.p[buf][P_M][t];
             const uint32_t idw = S.id[buf][t];
@@ -341,12 +343,29 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
     }
     cp_async_wait_all();
     if (flags) raise_flag(cnt, flags);
+    if (sc->adaptive_dt) {
+        for (int off = 16; off > 0; off >>= 1) v2max = fmax(v2max, __shfl_xor_sync(0xffffffffu, v2max, off));
+        if ((threadIdx.x & 31) == 0 && v2max > 0.0)
+            atomicMax(&cnt->vmax2_bits, (unsigned long long)__double_as_longlong(v2max));
+    }
 }
 
-// Advance the device clock after the substep's last reader of it (the grid kernel).
-__global__ void k_advance_time(Counters* cnt, const double* dt) {
-    cnt->time += *dt;
+// Advance the device clock after the substep's last reader of dt (G2P) and,
+// in adaptive mode, set the next substep's dt from the maximum particle speed
+// of this G2P: dt = min(dt_max, cfl dx / v_max) (MPMSimulator::computeDt,
+// Simulator.cpp:200-225, on the device instead of through a host read).
+template <typename R>
+__global__ void k_advance_time(Counters* cnt, SceneDev<R>* sc, SceneDev<double>* sc64) {
+    cnt->time += sc64->dt;
     cnt->substeps += 1;
+    if (sc64->adaptive_dt) {
+        const double vmax = sqrt(__longlong_as_double((long long)cnt->vmax2_bits));
+        double dt = sc64->dt_max;
+        if (vmax > 0 && sc64->cfl_dx / vmax < sc64->dt_max) dt = sc64->cfl_dx / vmax;
+        sc64->dt = dt;
+        sc->dt = (R)dt;
+        cnt->vmax2_bits = 0ull;
+    }
 }
 
 template <typename R>
@@ -364,7 +383,7 @@ cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, cons
     const int ctas = max(1, min(bin.nb_cap, cfg.num_sms * per_sm));
     k_g2p<R><<<ctas, kG2PUnit, sizeof(G2PShared<R>), stream>>>(sc, fallback64, in, out, aux, bin,
                                                reinterpret_cast<const R*>(grid.nodes), cnt);
-    k_advance_time<<<1, 1, 0, stream>>>(cnt, &sc64->dt);
+    k_advance_time<R><<<1, 1, 0, stream>>>(cnt, const_cast<SceneDev<R>*>(sc), const_cast<SceneDev<double>*>(sc64));
     return cudaGetLastError();
 }
 

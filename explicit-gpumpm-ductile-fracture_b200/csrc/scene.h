@@ -45,6 +45,9 @@ struct SceneBase {
     // Launch shapes are sized for this many SMs (0: the whole device).
     virtual void set_sm_share(int sms) = 0;
     virtual int sm_share() const = 0;
+
+    // Checkpoint of the particle state and clock (gmpm_scene_save).
+    virtual gmpm_status save(const char* path) = 0;
 };
 
 }  // namespace gmpm

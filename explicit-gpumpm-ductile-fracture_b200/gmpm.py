@@ -18,9 +18,9 @@ MAX_SPHERE_BCS = 2
 MAX_MATERIALS = 8
 
 # gmpm_status
-OK, INVALID_ARG, OOM, TABLE_OVERFLOW, NONFINITE, OUT_OF_DOMAIN, CUDA_ERROR, NOT_SUPPORTED, NO_DEVICE = range(9)
+OK, INVALID_ARG, OOM, TABLE_OVERFLOW, NONFINITE, OUT_OF_DOMAIN, CUDA_ERROR, NOT_SUPPORTED, NO_DEVICE, IO_ERROR = range(10)
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "TABLE_OVERFLOW", 4: "NONFINITE", 5: "OUT_OF_DOMAIN",
-                6: "CUDA_ERROR", 7: "NOT_SUPPORTED", 8: "NO_DEVICE"}
+                6: "CUDA_ERROR", 7: "NOT_SUPPORTED", 8: "NO_DEVICE", 9: "IO_ERROR"}
 
 FLAG_OUT_OF_DOMAIN, FLAG_NONFINITE, FLAG_SVD_NOCONVERGE, FLAG_TABLE_OVERFLOW, FLAG_COPY_TIMEOUT = 1, 2, 4, 8, 16
 
@@ -64,7 +64,8 @@ class SceneDesc(C.Structure):
                 ("wall_layers", C.c_int32), ("n_slab_bcs", C.c_int32), ("n_sphere_bcs", C.c_int32),
                 ("slabs", SlabBC * MAX_SLAB_BCS), ("spheres", SphereBC * MAX_SPHERE_BCS),
                 ("precision", C.c_int32), ("phase_field", C.c_int32), ("deterministic", C.c_int32),
-                ("block_capacity", C.c_int32), ("svd_fallback_ratio", C.c_double)]
+                ("block_capacity", C.c_int32), ("svd_fallback_ratio", C.c_double),
+                ("adaptive_dt", C.c_int32), ("_pad2", C.c_int32), ("cfl_number", C.c_double)]
 
 
 class ParticleInit(C.Structure):
@@ -77,14 +78,15 @@ class Diag(C.Structure):
                 ("grid_momentum", C.c_double * 3), ("kinetic_energy", C.c_double), ("max_speed", C.c_double),
                 ("min_damage", C.c_double), ("time", C.c_double), ("substeps", C.c_int64),
                 ("n_particles", C.c_int64), ("n_blocks", C.c_int32), ("n_grid_blocks", C.c_int32),
-                ("flags", C.c_uint32), ("_pad0", C.c_int32), ("kernel_launches", C.c_int64)]
+                ("flags", C.c_uint32), ("_pad0", C.c_int32), ("kernel_launches", C.c_int64), ("dt", C.c_double)]
 
     def as_dict(self) -> dict:
         return dict(particle_mass=self.particle_mass, particle_momentum=list(self.particle_momentum),
                     grid_mass=self.grid_mass, grid_momentum=list(self.grid_momentum),
                     kinetic_energy=self.kinetic_energy, max_speed=self.max_speed, min_damage=self.min_damage,
                     time=self.time, substeps=self.substeps, n_particles=self.n_particles, n_blocks=self.n_blocks,
-                    n_grid_blocks=self.n_grid_blocks, flags=self.flags, kernel_launches=self.kernel_launches)
+                    n_grid_blocks=self.n_grid_blocks, flags=self.flags, kernel_launches=self.kernel_launches,
+                    dt=self.dt)
 
 
 class StageTimes(C.Structure):
@@ -164,6 +166,8 @@ SIGNATURES = {
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
     "gmpm_generate_particles": (C.c_int, [C.POINTER(Geometry), C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                           C.POINTER(C.c_int32), C.c_int64]),
+    "gmpm_scene_save": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "gmpm_scene_load": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
     "gmpm_batch_options_defaults": (None, [C.POINTER(BatchOptions)]),
     "gmpm_batch_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.POINTER(BatchOptions),
                                     C.POINTER(C.c_void_p)]),
@@ -287,6 +291,22 @@ class Scene:
 
     def substep(self, n: int = 1, stream: int | None = None) -> None:
         check(lib().gmpm_substep(self.h, int(n), C.c_void_p(stream) if stream else None), "substep")
+
+    def save(self, path) -> None:
+        check(lib().gmpm_scene_save(self.h, str(path).encode()), "scene_save")
+
+    @classmethod
+    def load(cls, ctx: Context, path) -> "Scene":
+        """A scene restored from a checkpoint written by save()."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        check(lib().gmpm_scene_load(ctx.h, str(path).encode(), C.byref(self.h)), "scene_load")
+        d = Diag()
+        check(lib().gmpm_diagnostics(self.h, C.byref(d)), "diagnostics")
+        self.n = int(d.n_particles)
+        self.desc = None
+        return self
 
     def substep_timed(self, n: int = 1, stream: int | None = None) -> dict:
         t = StageTimes()

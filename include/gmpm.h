@@ -40,7 +40,8 @@ typedef enum gmpm_status {
     GMPM_OUT_OF_DOMAIN = 5,    /* particle stencil left the grid (reference quirk: negative base node) */
     GMPM_CUDA_ERROR = 6,
     GMPM_NOT_SUPPORTED = 7,
-    GMPM_NO_DEVICE = 8
+    GMPM_NO_DEVICE = 8,
+    GMPM_IO_ERROR = 9          /* a checkpoint file could not be written, read or recognised */
 } gmpm_status;
 
 /* Device-side status flags accumulated during substeps (gmpm_diagnostics.flags). */
@@ -132,6 +133,11 @@ typedef struct gmpm_scene_desc {
     int32_t deterministic;     /* 1 = fixed-order P2G (bitwise reproducible), 0 = atomic fast mode */
     int32_t block_capacity;    /* max active pages; 0 = derive from the particle count */
     double svd_fallback_ratio; /* sigma_min/sigma_max threshold for the FP64 fallback (1e-3) */
+    int32_t adaptive_dt;       /* 1: each substep's dt = min(dt, cfl_number dx / max |v_p|), computed on the
+                                  device from the previous G2P's velocities (MPMSimulator::computeDt,
+                                  Simulator.cpp:200-225, without its host read); dt is then the upper bound */
+    int32_t _pad2;
+    double cfl_number;         /* 0.3f as in computeDt (default) */
 } gmpm_scene_desc;
 
 /* Initial particle state.  Replaces the h_pos/h_vel/h_mass arrays handed to
@@ -205,6 +211,7 @@ typedef struct gmpm_diag {
     uint32_t flags;            /* GMPM_FLAG_* accumulated since creation */
     int32_t _pad0;
     int64_t kernel_launches;   /* kernels this scene launched since creation */
+    double dt;                 /* time step of the next substep */
 } gmpm_diag;
 
 /* Per-stage device time of gmpm_substep_timed, summed over its substeps
@@ -360,6 +367,15 @@ typedef struct gmpm_scene_geometry {
 
 gmpm_status gmpm_generate_particles(const gmpm_scene_geometry* geom, int64_t* count,
                                     double* positions, int32_t* material_ids, int64_t capacity);
+
+/* ---- Checkpoint / resume ------------------------------------------------------------------------
+ * A binary snapshot of a scene: its description, clock (time, substeps, current dt) and every particle
+ * plane of the state in the internal order (the reference's Attribs_Back_Host, Particles.cpp:33-52,
+ * and its declared but undefined writePartio, Simulator.h:35, as a restartable file).  Binning and grid
+ * are rebuilt by the next substep, so a loaded scene continues bitwise like the original in
+ * deterministic mode.  The file is tied to the library's struct layouts (native byte order). */
+gmpm_status gmpm_scene_save(gmpm_scene* scene, const char* path);
+gmpm_status gmpm_scene_load(gmpm_context* ctx, const char* path, gmpm_scene** out);
 
 /* ---- Batched stepping of independent scenes --------------------------------------------------
  * No reference counterpart: the reference steps one scene per MPMSimulator::simulateStick call

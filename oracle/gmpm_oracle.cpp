@@ -696,6 +696,7 @@ struct orc_scene {
     double grid_mass = 0, grid_mom[3] = {0, 0, 0};
     double time = 0;
     int64_t substeps = 0;
+    double dt_max = 0;  // the scene's dt (upper bound of the adaptive step)
     uint32_t flags = 0;
 };
 
@@ -1109,6 +1110,7 @@ orc_scene* orc_scene_create(const gmpm_scene_desc* desc, int64_t n, const double
     if (!desc || n <= 0 || !pos || !mass) return nullptr;
     orc_scene* s = new orc_scene();
     s->desc = *desc;
+    s->dt_max = desc->dt;
     s->n = n;
     s->dx = desc->dx;
     s->inv_dx = 1.0 / desc->dx;
@@ -1145,9 +1147,26 @@ void orc_scene_destroy(orc_scene* s) { delete s; }
 
 uint32_t orc_rebin(orc_scene* s) { return rebin(*s); }
 
+// CFL step of MPMSimulator::computeDt (Simulator.cpp:200-225): the maximum
+// particle speed (calVelSqur + mymaxF, Particle_kernal.cu:421-440) bounds dt
+// by dx * 0.3f / v_max, with the scene's dt as the upper bound.
+static double cfl_dt(const orc_scene& s) {
+    double v2max = 0.0;
+    for (int64_t p = 0; p < s.n; ++p) {
+        const double* v = &s.v[3 * p];
+        v2max = std::max(v2max, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+    const double vmax = std::sqrt(v2max);
+    const double cfl = s.desc.cfl_number > 0 ? s.desc.cfl_number : (double)0.3f;
+    double dt = s.dt_max;
+    if (vmax > 0 && (s.dx * cfl) / vmax < s.dt_max) dt = (s.dx * cfl) / vmax;
+    return dt;
+}
+
 uint32_t orc_substep(orc_scene* s, int n) {
     uint32_t fl = 0;
     for (int it = 0; it < n; ++it) {
+        if (s->desc.adaptive_dt) s->desc.dt = cfl_dt(*s);
         fl |= rebin(*s);
         p2g(*s);
         grid_update(*s);
@@ -1247,6 +1266,7 @@ void orc_diagnostics(const orc_scene* s, gmpm_diag* d) {
     d->min_damage = cmin;
     d->time = s->time;
     d->substeps = s->substeps;
+    d->dt = s->desc.adaptive_dt ? cfl_dt(*s) : s->desc.dt;
     d->n_particles = s->n;
     d->n_blocks = (int32_t)s->block_keys.size();
     d->n_grid_blocks = (int32_t)s->grid_keys.size();

@@ -61,7 +61,7 @@ def test_struct_layouts_match_header(pkg, tmp_path):
 
 def test_status_strings(pkg):
     L = pkg.gmpm.lib()
-    for s in range(9):
+    for s in range(10):
         assert L.gmpm_status_string(s)
     assert L.gmpm_status_string(0) == b"ok"
 

@@ -113,3 +113,20 @@ def test_fp32_with_fp64_svd_fallback(pkg, ctx, oracle):
         print(f"\n[plates32 prec={prec} 30 substeps] {format_errors(res[prec])}")
     for k in CORE:
         assert res[G.PRECISION_FP32_FP64SVD][k] <= 2 * res[G.PRECISION_FP32][k] + 1e-7
+
+
+def test_adaptive_dt_matches_oracle(pkg, ctx, oracle):
+    """Adaptive (CFL) time step computed on the device from G2P's maximum speed:
+    FP64 GPU and oracle take the same steps and agree to 1e-9."""
+    G = pkg.gmpm
+    sp = pkg.scenes.blob(n_side=8, velocity=(3.0, -2.0, 1.0), precision=G.PRECISION_FP64)
+    sp.desc.dt = 5e-3
+    sp.desc.adaptive_dt = 1
+    gpu, orc = run_pair(pkg, ctx, oracle, sp, 10)
+    dg, do = gpu.diagnostics(), orc.diagnostics(G.Diag)
+    assert dg["dt"] < 5e-3 and dg["dt"] == pytest.approx(do["dt"], rel=1e-12)
+    assert dg["time"] == pytest.approx(do["time"], rel=1e-12)
+    e = errors(G, gpu, orc, sp.positions, dx=sp.desc.dx, fields=CORE)
+    print(f"\n[blob adaptive dt FP64 10 substeps] dt={dg['dt']:.6g} {format_errors(e)}")
+    for k in CORE:
+        assert e[k] <= 1e-9, (k, e[k])

@@ -126,3 +126,23 @@ def test_oracle_is_deterministic(pkg, oracle):
     b.substep(5)
     for f in range(12):
         assert np.array_equal(a.field(f), b.field(f)), f
+
+
+def test_adaptive_dt_follows_cfl_bound(pkg, oracle):
+    """Adaptive mode: each substep's dt is min(dt, 0.3f dx / max |v_p|) of the
+    velocities entering it (MPMSimulator::computeDt, Simulator.cpp:200-225)."""
+    G = pkg.gmpm
+    sp = pkg.scenes.blob(n_side=6, velocity=(3.0, -2.0, 1.0), precision=G.PRECISION_FP64)
+    sp.desc.dt = 5e-3
+    sp.desc.adaptive_dt = 1
+    o = oracle.OracleScene(sp.desc, sp.positions, sp.masses, sp.velocities, sp.material_ids)
+    t = 0.0
+    for _ in range(4):
+        v = o.field_by_id(G.FIELD["velocity"]).reshape(-1, 3)
+        vmax = float(np.sqrt(np.max(np.sum(v * v, axis=1))))
+        want = min(5e-3, sp.desc.dx * float(np.float32(0.3)) / vmax)
+        assert want < 5e-3
+        assert o.diagnostics(G.Diag)["dt"] == pytest.approx(want, rel=1e-15)
+        o.substep(1)
+        t += want
+        assert o.diagnostics(G.Diag)["time"] == pytest.approx(t, rel=1e-14)
