@@ -196,6 +196,9 @@ def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
     dev = torch.device("cuda", local_rank)
     ctx = G.Context(local_rank)
     sp, what = workload(pkg, args.workload)
+    if getattr(args, "implicit", False):
+        sp.desc.phase_field = G.PHASE_FIELD_IMPLICIT
+        what += ", implicit phase field (Jacobi-PCG, tol 1e-6, <= 100 iterations)"
     t0 = time.perf_counter()
     scene = sp.build(ctx)
     build_s = time.perf_counter() - t0
@@ -389,6 +392,8 @@ def main():
     ap.add_argument("--duration", type=float, default=600.0, help="served workload: seconds of arrivals")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload object of the line")
+    ap.add_argument("--implicit", action="store_true",
+                    help="the reference's implicit (Jacobi-PCG) phase field instead of the explicit update")
     ap.add_argument("--no-served", action="store_true", help="skip the served-workload object of the line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

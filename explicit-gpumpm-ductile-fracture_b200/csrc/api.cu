@@ -168,6 +168,8 @@ void fill_scene_dev(const gmpm_scene_desc& d, int key_bits, SceneDev<R>& s) {
     s.dx_d = d.dx;
     s.inv_dx_d = 1.0 / d.dx;
     s.adaptive_dt = d.adaptive_dt;
+    s.pcg_max_combine = d.pcg_max_combine;
+    s.pcg_tolerance = d.pcg_tolerance;
     s.dt_max = d.dt;
     s.cfl_dx = d.dx * (d.cfl_number > 0 ? d.cfl_number : (double)0.3f);
 }
@@ -205,7 +207,10 @@ gmpm_status validate(const gmpm_scene_desc* d, const gmpm_particle_init* init) {
     for (int q = 0; q < d->n_slab_bcs; ++q)
         if (d->slabs[q].axis < 0 || d->slabs[q].axis > 2) return GMPM_INVALID_ARG;
     if (d->precision < 0 || d->precision > 2) return GMPM_INVALID_ARG;
-    if (d->phase_field < 0 || d->phase_field > 1) return GMPM_INVALID_ARG;
+    if (d->phase_field < 0 || d->phase_field > 2) return GMPM_INVALID_ARG;
+    if (d->phase_field == GMPM_PHASE_FIELD_IMPLICIT &&
+        (d->pcg_max_iterations < 1 || d->pcg_max_iterations > 10000 || !(d->pcg_tolerance >= 0)))
+        return GMPM_INVALID_ARG;
     if (d->block_capacity < 0) return GMPM_INVALID_ARG;
     if (d->adaptive_dt < 0 || d->adaptive_dt > 1 || !(d->cfl_number >= 0)) return GMPM_INVALID_ARG;
     if (init->material_ids)
@@ -257,6 +262,7 @@ struct Scene : SceneBase {
 
     ~Scene() override {
         for (void* p : allocs) cudaFree(p);
+        if (pcg_done_host) cudaFreeHost(pcg_done_host);
         if (staging) cudaFree(staging);
         if (bc_staging) cudaFreeHost(bc_staging);
         if (dt_staging) cudaFreeHost(dt_staging);
@@ -278,8 +284,11 @@ struct Scene : SceneBase {
     }
 
     LaunchCfg cfg() const {
-        return LaunchCfg{share_ > 0 ? std::min(share_, ctx->num_sms) : ctx->num_sms, desc.deterministic};
+        return LaunchCfg{share_ > 0 ? std::min(share_, ctx->num_sms) : ctx->num_sms, desc.deterministic,
+                         desc.pcg_max_combine, desc.materials[0].mobility, desc.pcg_tolerance};
     }
+    bool implicit_pf() const { return desc.phase_field == GMPM_PHASE_FIELD_IMPLICIT; }
+    int* pcg_done_host = nullptr;  // pinned: the solve's done flag, read between iterations
 
     gmpm_status create(gmpm_context* c, const gmpm_scene_desc* d, const gmpm_particle_init* init) {
         ctx = c;
@@ -425,6 +434,20 @@ struct Scene : SceneBase {
         GMPM_TRY(alloc(&nodes, (size_t)ng_cap * kGridChannels * 64));
         grid.tile = tile;
         grid.nodes = nodes;
+        grid.pcg = PcgDev{};
+        if (implicit_pf()) {
+            const size_t nn = (size_t)ng_cap * 64;
+            PcgDev& P = grid.pcg;
+            for (double** v : {&P.x, &P.r, &P.mr, &P.s, &P.q, &P.d, &P.cg}) GMPM_TRY(alloc(v, nn));
+            GMPM_TRY(alloc(&P.tag, nn));
+            GMPM_TRY(alloc(&P.col, (size_t)3 * n));
+            P.nparts_cap = (int64_t)(nn / 128 + 1);
+            GMPM_TRY(alloc(&P.part, (size_t)3 * P.nparts_cap));
+            GMPM_TRY(alloc(&P.scal, 1));
+            GMPM_TRY(cudaMemset(P.scal, 0, sizeof(PcgScalars)));
+            P.n = n;
+            GMPM_TRY(cudaMallocHost(reinterpret_cast<void**>(&pcg_done_host), sizeof(int)));
+        }
         GMPM_TRY(prepare_p2g<R>());
         GMPM_TRY(prepare_g2p<R>());
         GMPM_TRY(cudaMemset(d_cnt, 0, sizeof(Counters)));
@@ -460,14 +483,34 @@ struct Scene : SceneBase {
     }
 
     // Kernels of one substep from state buffer c; ev (optional) receives
-    // events after bin, p2g, grid, g2p.  Host bookkeeping is left alone.
-    gmpm_status launch_one(cudaStream_t s, int c, cudaEvent_t* ev) {
+    // events after bin, p2g, grid (incl. an implicit phase-field solve), g2p.
+    // Host bookkeeping is left alone.  host_checks: the implicit solve reads
+    // its done flag every 4 iterations and stops launching (not when capturing).
+    gmpm_status launch_one(cudaStream_t s, int c, cudaEvent_t* ev, bool host_checks = true,
+                           int64_t* kernels = nullptr) {
         const LaunchCfg lc = cfg();
+        int64_t nk = kBinningKernels + 4;
         GMPM_TRY(launch_binning<R>(d_sc, st[c], bin, scan, d_cnt, lc.num_sms, s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[0], s));
         GMPM_TRY(launch_p2g<R>(d_sc, st[c], aux, bin, grid, d_cnt, lc, s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[1], s));
         GMPM_TRY(launch_grid<R>(d_sc, bin, grid, d_cnt, lc, s));
+        if (implicit_pf()) {
+            GMPM_TRY(launch_pcg_init<R>(d_sc, bin, grid, d_cnt, lc, s));
+            nk += kPcgInitKernels + kPcgFinishKernels;
+            for (int it = 0; it < desc.pcg_max_iterations; ++it) {
+                GMPM_TRY(launch_pcg_iteration<R>(d_sc, st[c], aux, bin, grid, d_cnt, lc, s));
+                nk += kPcgIterationKernels;
+                if (host_checks && (it & 3) == 3) {
+                    GMPM_TRY(cudaMemcpyAsync(pcg_done_host, &grid.pcg.scal->done, sizeof(int),
+                                             cudaMemcpyDeviceToHost, s));
+                    GMPM_TRY(cudaStreamSynchronize(s));
+                    if (*pcg_done_host) break;
+                }
+            }
+            GMPM_TRY(launch_pcg_finish<R>(d_sc, bin, grid, d_cnt, lc, s));
+        }
+        if (kernels) *kernels = nk;
         if (ev) GMPM_TRY(cudaEventRecord(ev[2], s));
         GMPM_TRY(launch_g2p<R>(d_sc, d_sc64, desc.precision == GMPM_PRECISION_FP32_FP64SVD ? d_sc64 : nullptr,
                                st[c], st[1 - c], aux, bin, grid, d_cnt, lc, s));
@@ -476,9 +519,11 @@ struct Scene : SceneBase {
     }
 
     gmpm_status one_substep(cudaStream_t s, cudaEvent_t* ev) {
-        gmpm_status r = launch_one(s, cur, ev);
+        int64_t nk = 0;
+        gmpm_status r = launch_one(s, cur, ev, true, &nk);
         if (r != GMPM_OK) return r;
         commit_substeps(1);
+        launches += nk - kernels_per_substep();
         return GMPM_OK;
     }
 
@@ -488,13 +533,17 @@ struct Scene : SceneBase {
     int64_t particles() const override { return n; }
     size_t device_bytes() const override { return dev_bytes_; }
     int parity() const override { return cur; }
-    int kernels_per_substep() const override { return kBinningKernels + 4; }
+    int kernels_per_substep() const override {
+        return kBinningKernels + 4 +
+               (implicit_pf() ? kPcgInitKernels + kPcgFinishKernels + desc.pcg_max_iterations * kPcgIterationKernels
+                              : 0);
+    }
     gmpm_status launch_substep(cudaStream_t s, int c) override {
         if (c != 0 && c != 1) return GMPM_INVALID_ARG;
-        return launch_one(s, c, nullptr);
+        return launch_one(s, c, nullptr, false);
     }
     void commit_substeps(int nsub) override {
-        launches += (int64_t)nsub * (kBinningKernels + 4);  // binning, p2g, grid, g2p, clock advance
+        launches += (int64_t)nsub * kernels_per_substep();  // as launched by a captured substep
         if (nsub & 1) cur = 1 - cur;
         binned = false;
     }
@@ -718,6 +767,7 @@ struct Scene : SceneBase {
         out->flags = h.flags;
         out->kernel_launches = launches;
         GMPM_TRY(cudaMemcpy(&out->dt, &d_sc64->dt, sizeof(double), cudaMemcpyDeviceToHost));
+        out->pcg_iterations = h.pcg_iterations;
         return GMPM_OK;
     }
 
@@ -898,6 +948,9 @@ gmpm_status gmpm_scene_desc_reference_defaults(gmpm_scene_desc* d, double dx, in
     d->svd_fallback_ratio = 1e-3;
     d->adaptive_dt = 0;
     d->cfl_number = (double)0.3f;                  // Simulator.cpp:211
+    d->pcg_max_iterations = 100;                   // ExplicitTimeIntegrator.cu:925
+    d->pcg_max_combine = 0;
+    d->pcg_tolerance = (double)1e-6f;              // :926 (float literal)
     return GMPM_OK;
 }
 

@@ -72,6 +72,8 @@ struct SceneDev {
     Real mobility;          // scene mobility used by the grid phase-field update (material 0)
     double dx_d, inv_dx_d;  // binning arithmetic is always FP64
     int adaptive_dt;        // CFL time step from the previous G2P's max speed
+    int pcg_max_combine;    // implicit phase field: combine partial dot products by max (reference quirk)
+    double pcg_tolerance;   // implicit phase field: stop when max |r| < tolerance
     double dt_max;          // the scene's dt: upper bound of the adaptive step
     double cfl_dx;          // cfl_number * dx
 };
@@ -85,6 +87,8 @@ struct Counters {
     double time;
     long long substeps;
     unsigned long long vmax2_bits;  // max |v_p|^2 of the last G2P (FP64 bits; non-negative, so integer order)
+    int pcg_iterations;             // implicit phase field: iterations of the last solve
+    int pad2;
 };
 
 // ---- SPGrid page keys -----------------------------------------------------

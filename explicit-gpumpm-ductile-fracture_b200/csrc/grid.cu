@@ -6,6 +6,7 @@
 //   * explicit phase-field update replacing the reference's Jacobi-PCG solve
 //     (ExplicitTimeIntegrator.cu:909-972):
 //       c_new = (M_L (c/dt + M) - M K c~) / (M_L/dt + M sum V w FP),
+//     or, in the implicit mode, the initial vectors of that solve (pcg.cu),
 //   * velocity conditions (generalised PullGrid_kernal, TimeIntegrator.cu:169-261)
 //     and the sticky walls of collideWithGround (TimeIntegrator.cu:117-165).
 // Writes v (3), dc = c_new - c (update_grid_phase, ExplicitTimeIntegrator.cu:632-642)
@@ -21,7 +22,7 @@ constexpr int kGridThreads = 256;  // 4 grid pages per CTA
 template <typename R>
 __global__ void __launch_bounds__(kGridThreads)
     k_grid(const SceneDev<R>* __restrict__ sc, BinDev bin, const R* __restrict__ tile, R* __restrict__ nodes,
-           double* __restrict__ diag, Counters* cnt) {
+           double* __restrict__ diag, PcgDev pcg, Counters* cnt) {
     const int ng = min(cnt->n_grid_blocks, bin.ng_cap);
     const int node = threadIdx.x & 63;
     const int ci = node >> 4, cj = (node >> 2) & 3, ck = node & 3;
@@ -55,7 +56,26 @@ __global__ void __launch_bounds__(kGridThreads)
             R v[3] = {ch[CH_P0] * im + sc->gravity[0] * dt, ch[CH_P1] * im + sc->gravity[1] * dt,
                       ch[CH_P2] * im + sc->gravity[2] * dt};
             R cnew = cgrid;
-            if (sc->phase_field) {
+            if (sc->phase_field == GMPM_PHASE_FIELD_IMPLICIT) {
+                // the solve's vectors (ExplicitTimeIntegrator.cu:913-935): rhs sum_p V w (c/dt + M)
+                // (volP2G_APIC) as r with x0 = 0, Jacobi diagonal sum_p V w (FP M + 1/dt)
+                // (preConditionP2G_APIC), mr = r / diag (precondition_subd), s = mr
+                const PcgDev& P = pcg;
+                const int64_t i = (int64_t)g * 64 + node;
+                const double Md = (double)Mob, dtd = (double)dt;
+                const double cg = (double)cgrid;
+                const double dg = Md * (double)ch[CH_VWFP] + (double)ch[CH_VW] / dtd;
+                const double b = (double)ch[CH_VW] * (cg / dtd + Md);
+                const double mr = fabs(dg) >= 1e-30 ? b / dg : 0.0;
+                P.x[i] = 0.0;
+                P.r[i] = b;
+                P.mr[i] = mr;
+                P.s[i] = mr;
+                P.q[i] = 0.0;
+                P.d[i] = dg;
+                P.cg[i] = cg;
+                P.tag[i] = 1;
+            } else if (sc->phase_field == GMPM_PHASE_FIELD_EXPLICIT) {
                 const R diagv = ch[CH_VW] / dt + Mob * ch[CH_VWFP];
                 const R rhs = ch[CH_VW] * (cgrid / dt + Mob) - Mob * ch[CH_KC];
                 if (diagv != R(0)) cnew = rhs / diagv;
@@ -100,6 +120,11 @@ __global__ void __launch_bounds__(kGridThreads)
             out[GC_DC] = cnew - cgrid;
             out[GC_CN] = cnew;
         }
+        if (sc->phase_field == GMPM_PHASE_FIELD_IMPLICIT && !(mass > R(0))) {
+            const int64_t i = (int64_t)g * 64 + node;
+            pcg.x[i] = pcg.r[i] = pcg.mr[i] = pcg.s[i] = pcg.q[i] = pcg.d[i] = pcg.cg[i] = 0.0;
+            pcg.tag[i] = 0;
+        }
         R* N = nodes + (int64_t)g * kGridChannels * 64 + node;
 #pragma unroll
         for (int q = 0; q < kGridChannels; ++q) N[q * 64] = out[q];
@@ -126,7 +151,7 @@ cudaError_t launch_grid(const SceneDev<R>* sc, BinDev bin, GridDev grid, Counter
     cudaMemsetAsync(grid.diag, 0, 4 * sizeof(double), stream);
     const int ctas = max(1, min(bin.ng_cap / 4 + 1, cfg.num_sms * 8));
     k_grid<R><<<ctas, kGridThreads, 0, stream>>>(sc, bin, reinterpret_cast<const R*>(grid.tile),
-                                                 reinterpret_cast<R*>(grid.nodes), grid.diag, cnt);
+                                                 reinterpret_cast<R*>(grid.nodes), grid.diag, grid.pcg, cnt);
     return cudaGetLastError();
 }
 

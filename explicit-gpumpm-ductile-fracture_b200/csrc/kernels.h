@@ -8,15 +8,46 @@
 
 namespace gmpm {
 
+// Device scalars of the implicit phase-field solve.
+struct PcgScalars {
+    double rho_old, alpha, rate, norm;
+    int done;        // converged, blew up or capped: later kernels of the solve return at once
+    int blowup;      // rho_old == 0: the reference sets x = 1e20 everywhere
+    int iterations;  // iterations of the current solve
+    int pad;
+};
+
+// Vectors of the implicit phase-field solve, FP64 over the grid nodes
+// (ng_cap * 64, in grid-page order), and the per-particle col vectors.
+struct PcgDev {
+    double* x;
+    double* r;
+    double* mr;
+    double* s;
+    double* q;
+    double* d;     // Jacobi diagonal sum_p V w (FP M + 1/dt)
+    double* cg;    // c_grid = sum w c / sum w
+    uint8_t* tag;  // node touched by a particle
+    double* col;   // [3][n] 4 L0^2 V grad s at the particles (sorted order)
+    double* part;  // [3][nparts_cap] partial sums over runs of 128 entries
+    PcgScalars* scal;
+    int64_t nparts_cap;
+    int64_t n;     // particles (col stride)
+};
+
 struct GridDev {
-    void* tile;        // [nb_cap][kP2GChannels][216] P2G page tiles (Real)
+    void* tile;        // [nb_cap][kP2GChannels][216] P2G page tiles (Real); also the solve's FP64 node tiles
     void* nodes;       // [ng_cap][kGridChannels][64] grid results (Real)
     double* diag;      // [8] FP64 accumulators: grid mass, grid momentum xyz, ...
+    PcgDev pcg;        // implicit phase field only (null pointers otherwise)
 };
 
 struct LaunchCfg {
     int num_sms;
     int deterministic;
+    int pcg_max_combine;   // implicit phase field settings
+    double pcg_mobility;
+    double pcg_tolerance;
 };
 
 template <typename R>
@@ -51,6 +82,19 @@ template <typename R>
 cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, const SceneDev<double>* fallback64,
                        const PState<R>& in, const PState<R>& out, const PAux<R>& aux, BinDev bin, GridDev grid,
                        Counters* cnt, LaunchCfg cfg, cudaStream_t stream);
+
+// Implicit phase field (pcg.cu): init after the grid kernel, one CG iteration
+// per call (kernels return at once after convergence), finish before G2P.
+template <typename R>
+cudaError_t launch_pcg_init(const SceneDev<R>* sc, BinDev bin, GridDev grid, Counters* cnt, LaunchCfg cfg,
+                            cudaStream_t stream);
+template <typename R>
+cudaError_t launch_pcg_iteration(const SceneDev<R>* sc, const PState<R>& st, const PAux<R>& aux, BinDev bin,
+                                 GridDev grid, Counters* cnt, LaunchCfg cfg, cudaStream_t stream);
+template <typename R>
+cudaError_t launch_pcg_finish(const SceneDev<R>* sc, BinDev bin, GridDev grid, Counters* cnt, LaunchCfg cfg,
+                              cudaStream_t stream);
+constexpr int kPcgInitKernels = 2, kPcgIterationKernels = 7, kPcgFinishKernels = 1;
 
 // Initial constitutive evaluation (F, c, alpha, psi given; g_old = 1).
 template <typename R>

@@ -26,7 +26,7 @@ FLAG_OUT_OF_DOMAIN, FLAG_NONFINITE, FLAG_SVD_NOCONVERGE, FLAG_TABLE_OVERFLOW, FL
 
 PRECISION_FP32, PRECISION_FP64, PRECISION_FP32_FP64SVD = 0, 1, 2
 HARDENING_EXPONENTIAL, HARDENING_LINEAR = 0, 1
-PHASE_FIELD_OFF, PHASE_FIELD_EXPLICIT = 0, 1
+PHASE_FIELD_OFF, PHASE_FIELD_EXPLICIT, PHASE_FIELD_IMPLICIT = 0, 1, 2
 
 FIELD = dict(position=0, velocity=1, F=2, B=3, damage=4, alpha=5, psi_max=6, stress=7, volume=8, FP=9,
              pf_flux=10, mass=11, id=12)
@@ -65,7 +65,8 @@ class SceneDesc(C.Structure):
                 ("slabs", SlabBC * MAX_SLAB_BCS), ("spheres", SphereBC * MAX_SPHERE_BCS),
                 ("precision", C.c_int32), ("phase_field", C.c_int32), ("deterministic", C.c_int32),
                 ("block_capacity", C.c_int32), ("svd_fallback_ratio", C.c_double),
-                ("adaptive_dt", C.c_int32), ("_pad2", C.c_int32), ("cfl_number", C.c_double)]
+                ("adaptive_dt", C.c_int32), ("_pad2", C.c_int32), ("cfl_number", C.c_double),
+                ("pcg_max_iterations", C.c_int32), ("pcg_max_combine", C.c_int32), ("pcg_tolerance", C.c_double)]
 
 
 class ParticleInit(C.Structure):
@@ -78,7 +79,8 @@ class Diag(C.Structure):
                 ("grid_momentum", C.c_double * 3), ("kinetic_energy", C.c_double), ("max_speed", C.c_double),
                 ("min_damage", C.c_double), ("time", C.c_double), ("substeps", C.c_int64),
                 ("n_particles", C.c_int64), ("n_blocks", C.c_int32), ("n_grid_blocks", C.c_int32),
-                ("flags", C.c_uint32), ("_pad0", C.c_int32), ("kernel_launches", C.c_int64), ("dt", C.c_double)]
+                ("flags", C.c_uint32), ("_pad0", C.c_int32), ("kernel_launches", C.c_int64), ("dt", C.c_double),
+                ("pcg_iterations", C.c_int32), ("_pad1", C.c_int32)]
 
     def as_dict(self) -> dict:
         return dict(particle_mass=self.particle_mass, particle_momentum=list(self.particle_momentum),
@@ -86,7 +88,7 @@ class Diag(C.Structure):
                     kinetic_energy=self.kinetic_energy, max_speed=self.max_speed, min_damage=self.min_damage,
                     time=self.time, substeps=self.substeps, n_particles=self.n_particles, n_blocks=self.n_blocks,
                     n_grid_blocks=self.n_grid_blocks, flags=self.flags, kernel_launches=self.kernel_launches,
-                    dt=self.dt)
+                    dt=self.dt, pcg_iterations=self.pcg_iterations)
 
 
 class StageTimes(C.Structure):

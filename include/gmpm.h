@@ -66,7 +66,10 @@ typedef enum gmpm_hardening {
 
 typedef enum gmpm_phase_field {
     GMPM_PHASE_FIELD_OFF = 0,
-    GMPM_PHASE_FIELD_EXPLICIT = 1     /* explicit diffusion, pointwise-implicit reaction */
+    GMPM_PHASE_FIELD_EXPLICIT = 1,    /* explicit diffusion, pointwise-implicit reaction */
+    GMPM_PHASE_FIELD_IMPLICIT = 2     /* the reference's Jacobi-preconditioned CG solve of
+                                         (D + M K) c = M_L (c_grid/dt + M) each substep
+                                         (ExplicitTimeIntegrator.cu:909-972) */
 } gmpm_phase_field;
 
 /* Material and fracture constants.  Replaces ElasticMaterial
@@ -138,6 +141,10 @@ typedef struct gmpm_scene_desc {
                                   Simulator.cpp:200-225, without its host read); dt is then the upper bound */
     int32_t _pad2;
     double cfl_number;         /* 0.3f as in computeDt (default) */
+    int32_t pcg_max_iterations; /* implicit phase field: iteration cap (100, ExplicitTimeIntegrator.cu:925) */
+    int32_t pcg_max_combine;   /* 1: dot products combine per-128-entry partial sums with max, as the
+                                  reference's getDotProduct does (quirk); 0: true sums (default) */
+    double pcg_tolerance;      /* stop when max |r| < tolerance (1e-6, :926) */
 } gmpm_scene_desc;
 
 /* Initial particle state.  Replaces the h_pos/h_vel/h_mass arrays handed to
@@ -212,6 +219,8 @@ typedef struct gmpm_diag {
     int32_t _pad0;
     int64_t kernel_launches;   /* kernels this scene launched since creation */
     double dt;                 /* time step of the next substep */
+    int32_t pcg_iterations;    /* implicit phase field: CG iterations of the last substep */
+    int32_t _pad1;
 } gmpm_diag;
 
 /* Per-stage device time of gmpm_substep_timed, summed over its substeps

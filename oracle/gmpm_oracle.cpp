@@ -698,6 +698,10 @@ struct orc_scene {
     int64_t substeps = 0;
     double dt_max = 0;  // the scene's dt (upper bound of the adaptive step)
     uint32_t flags = 0;
+    // implicit phase field: per grid node rhs, Jacobi diagonal, c_grid, tag; iterations of the last solve
+    std::vector<double> pcg_b, pcg_d, pcg_cg;
+    std::vector<uint8_t> pcg_tag;
+    int pcg_iterations = 0;
 };
 
 namespace {
@@ -874,6 +878,162 @@ void p2g(orc_scene& s) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Implicit phase field (ExplicitTimeIntegrator.cu:909-972)
+// ---------------------------------------------------------------------------
+
+// (K x)_i = sum_p grad w_ip . col_p with col_p = 4 L0^2 V_p sum_j grad w_jp x_j
+// (AxG2P_APIC, G2PKernal.cu:1006-1123, and the stiffness term of AxP2G_APIC,
+// P2GKernal.cu:1162-1326), summed per page tile in sorted particle order and
+// per grid node over the 8 overlapping tiles in slot order.
+void stiffness_apply(const orc_scene& s, const std::vector<double>& xv, std::vector<double>& out) {
+    const int64_t nb = (int64_t)s.block_keys.size(), ng = (int64_t)s.grid_keys.size();
+    const double dx = s.dx, inv_dx = s.inv_dx;
+    std::vector<double> tile(nb * 216, 0.0);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t b = 0; b < nb; ++b) {
+        double win[216];
+        for (int a = 0; a < 6; ++a)
+            for (int bb = 0; bb < 6; ++bb)
+                for (int cc = 0; cc < 6; ++cc) {
+                    const int d = ((a >> 2) << 2) | ((bb >> 2) << 1) | (cc >> 2);
+                    const int32_t g = s.adj[b * 8 + d];
+                    win[a * 36 + bb * 6 + cc] = g < 0 ? 0.0 : xv[(int64_t)g * 64 + (a & 3) * 16 + (bb & 3) * 4 + (cc & 3)];
+                }
+        double* T = &tile[b * 216];
+        for (int32_t p = s.block_start[b]; p < s.block_start[b + 1]; ++p) {
+            int base[3];
+            uint32_t f = 0;
+            base_node(s, &s.x[3 * p], base, &f);
+            double xp[3];
+            for (int a = 0; a < 3; ++a) xp[a] = s.x[3 * p + a] - base[a] * dx;
+            Weights W;
+            bspline(xp, inv_dx, W);
+            const int l0 = base[0] & 3, l1 = base[1] & 3, l2 = base[2] & 3;
+            double col[3] = {0, 0, 0};
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                    for (int k = 0; k < 3; ++k) {
+                        const double xn = win[(l0 + i) * 36 + (l1 + j) * 6 + (l2 + k)];
+                        col[0] += W.g[0][i] * W.w[1][j] * W.w[2][k] * xn;
+                        col[1] += W.w[0][i] * W.g[1][j] * W.w[2][k] * xn;
+                        col[2] += W.w[0][i] * W.w[1][j] * W.g[2][k] * xn;
+                    }
+            const double L0 = s.mc[s.mat[p]].m->length_scale;
+            const double para = s.vol[p] * 4.0 * L0 * L0;
+            for (int a = 0; a < 3; ++a) col[a] *= para;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                    for (int k = 0; k < 3; ++k) {
+                        const double hw = W.g[0][i] * W.w[1][j] * W.w[2][k] * col[0] +
+                                          W.w[0][i] * W.g[1][j] * W.w[2][k] * col[1] +
+                                          W.w[0][i] * W.w[1][j] * W.g[2][k] * col[2];
+                        T[(l0 + i) * 36 + (l1 + j) * 6 + (l2 + k)] += hw;
+                    }
+        }
+    }
+    out.assign(ng * 64, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < ng; ++q) {
+        const int gx = s.grid_base[3 * q], gy = s.grid_base[3 * q + 1], gz = s.grid_base[3 * q + 2];
+        int64_t src[8];
+        for (int d = 0; d < 8; ++d) {
+            const int sx = gx - (d >> 2), sy = gy - ((d >> 1) & 1), sz = gz - (d & 1);
+            src[d] = (sx < 0 || sy < 0 || sz < 0) ? -1 : find_block(s, page_key(sx, sy, sz));
+        }
+        for (int node = 0; node < 64; ++node) {
+            const int ci = node >> 4, cj = (node >> 2) & 3, ck = node & 3;
+            double v = 0.0;
+            for (int d = 0; d < 8; ++d) {
+                if (src[d] < 0) continue;
+                const int a = 4 * (d >> 2) + ci, b = 4 * ((d >> 1) & 1) + cj, c = 4 * (d & 1) + ck;
+                if (a >= 6 || b >= 6 || c >= 6) continue;
+                v += tile[src[d] * 216 + a * 36 + b * 6 + c];
+            }
+            out[q * 64 + node] = v;
+        }
+    }
+}
+
+// Dot product over the node vectors (myDotSum + mysumFm,
+// ExplicitTimeIntegrator.cu:573-610, 727-743): partial sums over consecutive
+// runs of 128 entries, combined by a sum, or by a maximum when the reference's
+// quirk is selected.
+double pcg_dot(const std::vector<double>& a, const std::vector<double>& b, bool max_combine) {
+    const int64_t n = (int64_t)a.size();
+    double total = 0.0, best = 0.0;
+    bool first = true;
+    for (int64_t k = 0; k < n; k += 128) {
+        double part = 0.0;
+        for (int64_t i = k; i < std::min(n, k + 128); ++i) part += a[i] * b[i];
+        total += part;
+        if (first || part > best) best = part;
+        first = false;
+    }
+    return max_combine ? best : total;
+}
+
+// max |r| (getNormSquare_b: max of squares, then sqrt; :711-725)
+double pcg_norm(const std::vector<double>& r) {
+    double m = 0.0;
+    for (double v : r) m = std::max(m, v * v);
+    return std::sqrt(m);
+}
+
+// The reference's Jacobi-preconditioned CG (ExplicitTimeIntegrator.cu:909-972)
+// for (D + M K) x = b on the tagged nodes, x0 = 0; then dc = x - c_grid
+// (update_grid_phase, :632-642).
+void pcg_phase_field(orc_scene& s) {
+    const int64_t N = (int64_t)s.pcg_b.size();
+    const double Mob = s.desc.materials[0].mobility;
+    const bool qmax = s.desc.pcg_max_combine != 0;
+    const int max_it = s.desc.pcg_max_iterations;
+    const double tol = s.desc.pcg_tolerance;
+    std::vector<double> x(N, 0.0), r(N, 0.0), mr(N, 0.0), sd(N, 0.0), q(N, 0.0), kx;
+    for (int64_t i = 0; i < N; ++i)
+        if (s.pcg_tag[i]) r[i] = s.pcg_b[i];
+    auto precondition = [&]() {  // precondition_subd (:677-700)
+        for (int64_t i = 0; i < N; ++i)
+            if (s.pcg_tag[i] && std::fabs(s.pcg_d[i]) >= 1e-30) mr[i] = r[i] / s.pcg_d[i];
+    };
+    precondition();
+    sd = mr;
+    double rho_old = pcg_dot(r, mr, qmax);
+    int it = 0;
+    for (; it < max_it; ++it) {
+        stiffness_apply(s, sd, kx);
+        for (int64_t i = 0; i < N; ++i) q[i] = s.pcg_tag[i] ? s.pcg_d[i] * sd[i] + Mob * kx[i] : 0.0;
+        const double sq = pcg_dot(sd, q, qmax);
+        const double alpha = rho_old / sq;
+        for (int64_t i = 0; i < N; ++i)
+            if (s.pcg_tag[i]) {
+                x[i] += sd[i] * alpha;
+                r[i] = r[i] - q[i] * alpha;
+            }
+        if (pcg_norm(r) < tol) {
+            ++it;
+            break;
+        }
+        precondition();
+        const double rho = pcg_dot(r, mr, qmax);
+        if (rho_old == 0.0) {
+            std::fill(x.begin(), x.end(), 1e20);
+            ++it;
+            break;
+        }
+        const double rate = rho / rho_old;
+        rho_old = rho;
+        for (int64_t i = 0; i < N; ++i)
+            if (s.pcg_tag[i]) sd[i] = sd[i] * rate + mr[i];
+    }
+    s.pcg_iterations = it;
+    for (int64_t i = 0; i < N; ++i)
+        if (s.pcg_tag[i]) {
+            s.gdc[i] = x[i] - s.pcg_cg[i];
+            s.gcn[i] = x[i];
+        }
+}
+
 // Grid stage for one node: undateGrid_kernal (TimeIntegrator.cu:63-111), the
 // explicit phase-field update, velocity conditions (PullGrid_kernal,
 // TimeIntegrator.cu:169-261, generalised) and the sticky walls of
@@ -886,6 +1046,13 @@ void grid_update(orc_scene& s) {
     const double dt = s.desc.dt, dx = s.dx, t_now = s.time;
     const double Mob = s.desc.materials[0].mobility;
     const bool pf = s.desc.phase_field == GMPM_PHASE_FIELD_EXPLICIT;
+    const bool pcg = s.desc.phase_field == GMPM_PHASE_FIELD_IMPLICIT;
+    if (pcg) {
+        s.pcg_b.assign(ng * 64, 0.0);
+        s.pcg_d.assign(ng * 64, 0.0);
+        s.pcg_cg.assign(ng * 64, 0.0);
+        s.pcg_tag.assign(ng * 64, 0);
+    }
     double gm = 0, gp0 = 0, gp1 = 0, gp2 = 0;
 #pragma omp parallel for schedule(static) reduction(+ : gm, gp0, gp1, gp2)
     for (int64_t q = 0; q < ng; ++q) {
@@ -929,6 +1096,14 @@ void grid_update(orc_scene& s) {
                 const double rhs = ch[CH_VW] * (cgrid / dt + Mob) - Mob * ch[CH_KC];
                 if (diag != 0.0) cnew = rhs / diag;
             }
+            if (pcg) {
+                // rhs sum_p V w (c_grid/dt + M) (volP2G_APIC, P2GKernal.cu:897-1030) and Jacobi
+                // diagonal sum_p V w (FP M + 1/dt) (preConditionP2G_APIC, :1032-1157)
+                s.pcg_b[gi] = ch[CH_VW] * (cgrid / dt + Mob);
+                s.pcg_d[gi] = Mob * ch[CH_VWFP] + ch[CH_VW] / dt;
+                s.pcg_cg[gi] = cgrid;
+                s.pcg_tag[gi] = 1;
+            }
             // velocity conditions
             const int I = 4 * gx + ci, J = 4 * gy + cj, K = 4 * gz + ck;
             const double pos[3] = {I * dx, J * dx, K * dx};
@@ -965,6 +1140,7 @@ void grid_update(orc_scene& s) {
     s.grid_mom[0] = gp0;
     s.grid_mom[1] = gp1;
     s.grid_mom[2] = gp2;
+    if (pcg) pcg_phase_field(s);
 }
 
 void stress_one(orc_scene& s, int64_t p) {
@@ -1267,6 +1443,7 @@ void orc_diagnostics(const orc_scene* s, gmpm_diag* d) {
     d->time = s->time;
     d->substeps = s->substeps;
     d->dt = s->desc.adaptive_dt ? cfl_dt(*s) : s->desc.dt;
+    d->pcg_iterations = s->pcg_iterations;
     d->n_particles = s->n;
     d->n_blocks = (int32_t)s->block_keys.size();
     d->n_grid_blocks = (int32_t)s->grid_keys.size();
