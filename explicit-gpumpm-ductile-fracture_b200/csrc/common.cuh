@@ -91,6 +91,15 @@ struct Counters {
     int pad2;
 };
 
+// Compensated (Kahan) summation: s += v with the low-order error carried in c.
+template <typename R>
+__device__ __forceinline__ void kahan_add(R& s, R& c, R v) {
+    const R y = v - c;
+    const R t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
 // ---- SPGrid page keys -----------------------------------------------------
 // The page key of block (bx,by,bz) is offset>>12 of SPGridMask::Linear_Offset:
 // Morton interleave with z in bit 0, y in bit 1, x in bit 2 (SPGridMask.cpp:97-105).

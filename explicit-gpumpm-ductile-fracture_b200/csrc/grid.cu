@@ -1,6 +1,7 @@
 // Grid stage, one thread per node of every grid page (active pages and their
 // "+" neighbours):
-//   * fixed-order sum of the (up to 8) P2G page tiles overlapping the page,
+//   * fixed-order, compensated (Kahan) sum of the (up to 8) P2G page tiles
+//     overlapping the page,
 //   * undateGrid_kernal (TimeIntegrator.cu:63-111): c = C/W, v = p/m + g dt
 //     (the force is already in p),
 //   * explicit phase-field update replacing the reference's Jacobi-PCG solve
@@ -31,9 +32,10 @@ __global__ void __launch_bounds__(kGridThreads)
     const double t_now = cnt->time;
     double dm = 0, dp0 = 0, dp1 = 0, dp2 = 0;
     for (int g = blockIdx.x * 4 + (threadIdx.x >> 6); g < ng; g += gridDim.x * 4) {
-        R ch[kP2GChannels];
+        // fixed-order, compensated sum of the page tiles overlapping the node
+        R ch[kP2GChannels], comp[kP2GChannels];
 #pragma unroll
-        for (int q = 0; q < kP2GChannels; ++q) ch[q] = R(0);
+        for (int q = 0; q < kP2GChannels; ++q) ch[q] = comp[q] = R(0);
 #pragma unroll
         for (int d = 0; d < 8; ++d) {
             const int a = 4 * (d >> 2) + ci, b = 4 * ((d >> 1) & 1) + cj, c = 4 * (d & 1) + ck;
@@ -42,7 +44,7 @@ __global__ void __launch_bounds__(kGridThreads)
             if (s < 0) continue;
             const R* T = tile + (int64_t)s * kP2GChannels * kWindowNodes + a * 36 + b * 6 + c;
 #pragma unroll
-            for (int q = 0; q < kP2GChannels; ++q) ch[q] += T[q * kWindowNodes];
+            for (int q = 0; q < kP2GChannels; ++q) kahan_add(ch[q], comp[q], T[q * kWindowNodes]);
         }
         R out[kGridChannels] = {R(0), R(0), R(0), R(0), R(0)};
         const R mass = ch[CH_M];

@@ -27,7 +27,7 @@
 // registers: no shuffles and no per-particle atomics.
 //
 // Deterministic mode: after a page's last chunk the column sums are gathered
-// per window node in a fixed order (at most 9 terms) and written once to the
+// per window node in a fixed order (at most 9 terms, compensated) and written once to the
 // page's tile in HBM, so results are bitwise reproducible.  Fast mode:
 // columns add into a shared tile with atomics.  The grid kernel sums the
 // eight page tiles overlapping each grid page in fixed slot order either way.
@@ -481,15 +481,15 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
             // column (a - cx, b - cy), cx then cy ascending, all channels at once
             if (t < kWindowNodes) {
                 const int na = t / 36, nbb = (t / 6) % 6, nc = t % 6;
-                R sum[kP2GChannels];
+                R sum[kP2GChannels], comp[kP2GChannels];
 #pragma unroll
-                for (int ch = 0; ch < kP2GChannels; ++ch) sum[ch] = R(0);
+                for (int ch = 0; ch < kP2GChannels; ++ch) sum[ch] = comp[ch] = R(0);
                 for (int cx = max(0, na - 2); cx <= min(3, na); ++cx)
                     for (int cy = max(0, nbb - 2); cy <= min(3, nbb); ++cy) {
                         const R* src =
                             acc_smem + ((cx * 4 + cy) * 9 + (na - cx) * 3 + (nbb - cy)) * kColAcc + nc * 9;
 #pragma unroll
-                        for (int ch = 0; ch < kP2GChannels; ++ch) sum[ch] += src[ch];
+                        for (int ch = 0; ch < kP2GChannels; ++ch) kahan_add(sum[ch], comp[ch], src[ch]);
                     }
 #pragma unroll
                 for (int ch = 0; ch < kP2GChannels; ++ch) out[ch * kWindowNodes + t] = sum[ch];

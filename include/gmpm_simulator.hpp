@@ -263,6 +263,13 @@ class MPMSimulator {
         getModelParticlePtr()->Attribs_Back_Host(h_pos, h_vel, h_indices);
     }
 
+    // Simulator.h:35 declares writePartio without a definition; here it writes
+    // a restartable checkpoint of the scene (gmpm_scene_save; gmpm_scene_load
+    // resumes it bitwise).
+    void writePartio(const std::string& filename) {
+        gmpm_check(gmpm_scene_save(scene_, filename.c_str()), "writePartio");
+    }
+
     std::unique_ptr<MPMTimeIntegrator>& getTimeIntegratorPtr() { return h_pTimeIntegrator; }
     std::unique_ptr<SPGrid>& getGridPtr() { return h_pGrid; }
     std::unique_ptr<DomainTransformer>& getTransformerPtr() { return h_pTrans; }
