@@ -16,6 +16,14 @@
 
 namespace gmpm {
 
+gmpm_status flags_status(unsigned int f) {
+    if (f & GMPM_FLAG_COPY_TIMEOUT) return GMPM_CUDA_ERROR;
+    if (f & GMPM_FLAG_TABLE_OVERFLOW) return GMPM_TABLE_OVERFLOW;
+    if (f & GMPM_FLAG_OUT_OF_DOMAIN) return GMPM_OUT_OF_DOMAIN;
+    if (f & GMPM_FLAG_NONFINITE) return GMPM_NONFINITE;
+    return GMPM_OK;
+}
+
 gmpm_status cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return GMPM_OK;
     if (e == cudaErrorMemoryAllocation) return GMPM_OOM;
@@ -260,10 +268,27 @@ struct Scene : SceneBase {
     // kernels per launch_binning: keys, 3 scans x 3, mark, 2 compactions, links, hist, scatter, canon
     static constexpr int kBinningKernels = 17;
 
+    // Device memory comes from the device's stream-ordered pool.  A scene
+    // released on a stream (the serving loop, after its last use there) frees
+    // it on that stream without synchronising the device; otherwise the
+    // device is synchronised first, since the scene's work may be in flight
+    // on any stream.
+    cudaStream_t release_stream_ = nullptr;
+    bool release_on_stream_ = false;
+    void set_release_stream(cudaStream_t s) override {
+        release_stream_ = s;
+        release_on_stream_ = true;
+    }
+
     ~Scene() override {
-        for (void* p : allocs) cudaFree(p);
+        cudaStream_t rs = release_stream_;
+        if (!release_on_stream_) {
+            cudaDeviceSynchronize();
+            rs = 0;
+        }
+        for (void* p : allocs) cudaFreeAsync(p, rs);
+        if (staging) cudaFreeAsync(staging, rs);
         if (pcg_done_host) cudaFreeHost(pcg_done_host);
-        if (staging) cudaFree(staging);
         if (bc_staging) cudaFreeHost(bc_staging);
         if (dt_staging) cudaFreeHost(dt_staging);
         for (cudaEvent_t e : dt_done)
@@ -275,7 +300,7 @@ struct Scene : SceneBase {
     template <typename T>
     cudaError_t alloc(T** p, size_t count) {
         void* q = nullptr;
-        cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
+        cudaError_t e = cudaMallocAsync(&q, count * sizeof(T) + 16, 0);
         if (e != cudaSuccess) return e;
         allocs.push_back(q);
         dev_bytes_ += count * sizeof(T) + 16;
@@ -329,7 +354,7 @@ struct Scene : SceneBase {
         const size_t nplanes = 2 * state_planes + aux_planes;
         const size_t plane_bytes = round_up((size_t)stride * sizeof(R), 256);
         const size_t id_bytes = round_up((size_t)stride * sizeof(uint32_t), 256);
-        GMPM_TRY(cudaMalloc(&pstore, nplanes * plane_bytes + 2 * id_bytes));
+        GMPM_TRY(cudaMallocAsync(&pstore, nplanes * plane_bytes + 2 * id_bytes, 0));
         allocs.push_back(pstore);
         dev_bytes_ += nplanes * plane_bytes + 2 * id_bytes;
         char* base = reinterpret_cast<char*>(pstore);
@@ -451,7 +476,9 @@ struct Scene : SceneBase {
         GMPM_TRY(prepare_p2g<R>());
         GMPM_TRY(prepare_g2p<R>());
         GMPM_TRY(cudaMemset(d_cnt, 0, sizeof(Counters)));
-        GMPM_TRY(cudaDeviceSynchronize());
+        // creation work ran on the legacy stream; waiting for it alone leaves
+        // other streams' work (e.g. a serving batch) running
+        GMPM_TRY(cudaStreamSynchronize(0));
         return GMPM_OK;
     }
 
@@ -687,10 +714,10 @@ struct Scene : SceneBase {
             return GMPM_OK;
         }
         if (staging_bytes < need) {
-            if (staging) cudaFree(staging);
+            if (staging) cudaFreeAsync(staging, s);
             staging = nullptr;
             staging_bytes = 0;
-            GMPM_TRY(cudaMalloc(&staging, need));
+            GMPM_TRY(cudaMallocAsync(&staging, need, s));
             staging_bytes = need;
         }
         GMPM_TRY(launch_pack_field<R>(st[cur], aux, field, dtype, order, n, staging, s));
@@ -839,6 +866,33 @@ struct Scene : SceneBase {
         return GMPM_OK;
     }
 
+    gmpm_status status_on_stream(cudaStream_t s) override {
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        Counters h{};
+        GMPM_TRY(cudaMemcpyAsync(&h, d_cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
+        GMPM_TRY(cudaStreamSynchronize(s));
+        return flags_status(h.flags);
+    }
+    gmpm_status enqueue_flags(unsigned int* dst, cudaStream_t s) override {
+        GMPM_TRY(cudaMemcpyAsync(dst, &d_cnt->flags, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        return GMPM_OK;
+    }
+    gmpm_status enqueue_read(int field, int dtype, int order, void* dst, cudaStream_t s) override {
+        const int nc = field_components(field);
+        if (nc == 0 || !dst || dtype < 0 || dtype > 2 || order < 0 || order > 1) return GMPM_INVALID_ARG;
+        const size_t need = (size_t)n * nc * (dtype == GMPM_DTYPE_F64 ? 8 : 4);
+        if (staging_bytes < need) {
+            if (staging) cudaFreeAsync(staging, s);
+            staging = nullptr;
+            staging_bytes = 0;
+            GMPM_TRY(cudaMallocAsync(&staging, need, s));
+            staging_bytes = need;
+        }
+        GMPM_TRY(launch_pack_field<R>(st[cur], aux, field, dtype, order, n, staging, s));
+        GMPM_TRY(cudaMemcpyAsync(dst, staging, need, cudaMemcpyDefault, s));
+        return GMPM_OK;
+    }
+
     gmpm_status sync() override {
         GMPM_TRY(cudaSetDevice(ctx->device));
         GMPM_TRY(cudaDeviceSynchronize());
@@ -902,6 +956,15 @@ gmpm_status gmpm_context_create(int device, gmpm_context** out) {
         return GMPM_CUDA_ERROR;
     }
     c->num_sms = c->prop.multiProcessorCount;
+    // Scenes allocate from the device's stream-ordered pool; keep freed memory
+    // cached in the pool (this process only) so scenes created after others
+    // were released reuse it without returning to the driver.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     *out = c;
     return GMPM_OK;
 }

@@ -335,3 +335,19 @@ gmpm_status gmpm_batch_destroy(gmpm_batch* b) {
 }
 
 }  // extern "C"
+
+namespace gmpm {
+// Destroy a batch whose graph launches may still run: executable graphs,
+// streams and events may be destroyed with work in flight (the driver
+// releases them when it completes), so no synchronisation is needed.  The
+// scenes' memory is untouched.
+void batch_destroy_deferred(gmpm_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->impl.ctx->device);
+    delete b;
+}
+}  // namespace gmpm
+
+extern "C" {
+
+}  // extern "C"

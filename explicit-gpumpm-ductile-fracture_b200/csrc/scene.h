@@ -48,7 +48,22 @@ struct SceneBase {
 
     // Checkpoint of the particle state and clock (gmpm_scene_save).
     virtual gmpm_status save(const char* path) = 0;
+
+    // Serving: status flags read on a stream (no device synchronisation), and
+    // release of the scene's memory on a stream after its last use there.
+    virtual gmpm_status status_on_stream(cudaStream_t s) = 0;
+    virtual void set_release_stream(cudaStream_t s) = 0;
+    // Enqueue (no wait) a read of one field into pinned or device memory, and
+    // of the status flags into pinned memory.
+    virtual gmpm_status enqueue_read(int field, int dtype, int order, void* dst, cudaStream_t s) = 0;
+    virtual gmpm_status enqueue_flags(unsigned int* dst, cudaStream_t s) = 0;
 };
+
+// Destroy a batch without synchronising the device (its graphs may still run).
+void batch_destroy_deferred(gmpm_batch* b);
+
+// Status of a set of device flags (GMPM_FLAG_*).
+gmpm_status flags_status(unsigned int flags);
 
 }  // namespace gmpm
 

@@ -11,12 +11,18 @@
 // reused.  Results do not depend on which scenes share a batch (bitwise in
 // deterministic mode).  No reference counterpart: the reference runs one
 // scene per process from its GLUT loop (gl_main.cpp:304-314).
+//
+// Threads: one thread steps the server; submit, poll, read, release and
+// stats may be called from other threads at the same time (a mutex guards
+// the queue, the request table and the counters; creating, advancing and
+// retiring scenes run outside it).
 #include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -62,7 +68,45 @@ struct Request {
     size_t est_bytes = 0, bytes = 0;
     double t_submit = 0, t_admit = 0, t_finish = 0;
     gmpm_scene* scene = nullptr;
-    std::map<int, std::vector<float>> results;
+    // final fields (FP32, original order) in a pinned buffer: position,
+    // velocity, F, damage at the offsets below, then the status flags
+    unsigned char* results = nullptr;
+    size_t results_bytes = 0;
+    size_t offset[4] = {0, 0, 0, 0};
+    unsigned int* flags = nullptr;
+    cudaEvent_t ready = nullptr;  // the reads of a retiring request have landed
+};
+
+// Reused pinned host buffers: allocating pinned memory can stall the device,
+// so buffers are kept and handed out again by size.
+struct PinnedPool {
+    std::multimap<size_t, unsigned char*> free_bufs;
+    std::vector<unsigned char*> all;
+    ~PinnedPool() {
+        for (unsigned char* p : all) cudaFreeHost(p);
+    }
+    unsigned char* acquire(size_t bytes, size_t* got) {
+        auto it = free_bufs.lower_bound(bytes);
+        if (it != free_bufs.end() && it->first <= 2 * bytes + (1u << 20)) {
+            unsigned char* p = it->second;
+            *got = it->first;
+            free_bufs.erase(it);
+            return p;
+        }
+        size_t sz = 1u << 20;
+        while (sz < bytes) sz <<= 1;
+        unsigned char* p = nullptr;
+        if (cudaMallocHost(reinterpret_cast<void**>(&p), sz) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        all.push_back(p);
+        *got = sz;
+        return p;
+    }
+    void release(unsigned char* p, size_t bytes) {
+        if (p) free_bufs.emplace(bytes, p);
+    }
 };
 
 // Device bytes of a scene before it exists: particle planes (55 words + 2 ids
@@ -82,9 +126,13 @@ size_t estimate_bytes(const gmpm_scene_desc& d, int64_t n) {
 struct Server {
     gmpm_context* ctx = nullptr;
     gmpm_server_options opt{};
+    std::mutex mu;  // reqs, queue, st and the request fields poll reads
     std::map<int64_t, std::unique_ptr<Request>> reqs;
     std::deque<int64_t> queue;
-    std::vector<int64_t> live;
+    std::vector<Request*> live;  // stepping thread only
+    std::vector<Request*> retiring;  // reads enqueued, waiting for their event (stepping thread only)
+    std::vector<cudaEvent_t> spare_events;
+    PinnedPool pinned;  // guarded by mu
     gmpm_batch* batch = nullptr;
     bool batch_stale = true;
     bool tuned = false;
@@ -95,6 +143,10 @@ struct Server {
     double t0 = now_s();
 
     ~Server() {
+        for (Request* r : retiring) cudaEventSynchronize(r->ready);
+        for (cudaEvent_t e : spare_events) cudaEventDestroy(e);
+        for (auto& kv : reqs)
+            if (kv.second->ready) cudaEventDestroy(kv.second->ready);
         if (batch) gmpm_batch_destroy(batch);
         batch = nullptr;
         for (auto& kv : reqs)
@@ -104,7 +156,10 @@ struct Server {
     void drop_batch() {
         if (batch) {
             gmpm_batch_info info;
-            if (gmpm_batch_get_info(batch, &info) == GMPM_OK) st.capture_microseconds += (int64_t)(info.capture_seconds * 1e6);
+            if (gmpm_batch_get_info(batch, &info) == GMPM_OK) {
+                std::lock_guard<std::mutex> lk(mu);
+                st.capture_microseconds += (int64_t)(info.capture_seconds * 1e6);
+            }
             // only the first batch is tuned: if it ends before tuning finished,
             // later batches keep the default launch shapes
             remember_tuning();
@@ -112,7 +167,7 @@ struct Server {
                 tuned = true;
                 tuned_opt = gmpm_batch_options{};
             }
-            gmpm_batch_destroy(batch);
+            batch_destroy_deferred(batch);
         }
         batch = nullptr;
         batch_stale = true;
@@ -123,7 +178,6 @@ struct Server {
             return GMPM_INVALID_ARG;
         auto r = std::unique_ptr<Request>(new (std::nothrow) Request());
         if (!r) return GMPM_OOM;
-        r->id = next_id++;
         r->desc = *d;
         r->n = init->count;
         r->pos.assign(init->positions, init->positions + 3 * init->count);
@@ -132,8 +186,10 @@ struct Server {
         if (init->material_ids) r->mat.assign(init->material_ids, init->material_ids + init->count);
         r->horizon = horizon;
         r->est_bytes = estimate_bytes(*d, init->count);
-        r->t_submit = now_s() - t0;
         if (opt.hbm_budget_bytes > 0 && r->est_bytes > (size_t)opt.hbm_budget_bytes) return GMPM_OOM;
+        std::lock_guard<std::mutex> lk(mu);
+        r->id = next_id++;
+        r->t_submit = now_s() - t0;
         *id = r->id;
         queue.push_back(r->id);
         reqs[r->id] = std::move(r);
@@ -143,54 +199,125 @@ struct Server {
 
     // Admit queued requests in arrival order while the budget allows.
     void admit() {
-        while (!queue.empty()) {
-            if (opt.max_live > 0 && (int)live.size() >= opt.max_live) break;
-            Request& r = *reqs[queue.front()];
-            if (opt.hbm_budget_bytes > 0 && used + r.est_bytes > (size_t)opt.hbm_budget_bytes) break;
-            queue.pop_front();
+        const double ta = now_s();
+        admit_inner();
+        std::lock_guard<std::mutex> lk(mu);
+        st.admit_microseconds += (int64_t)((now_s() - ta) * 1e6);
+    }
+    void admit_inner() {
+        for (;;) {
+            Request* rp = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (queue.empty()) return;
+                if (opt.max_live > 0 && (int)live.size() >= opt.max_live) return;
+                Request& r = *reqs[queue.front()];
+                if (opt.hbm_budget_bytes > 0 && used + r.est_bytes > (size_t)opt.hbm_budget_bytes) return;
+                queue.pop_front();
+                rp = &r;
+            }
+            Request& r = *rp;
             gmpm_particle_init init{r.n, r.pos.data(), r.vel.empty() ? nullptr : r.vel.data(), r.mass.data(),
                                     r.mat.empty() ? nullptr : r.mat.data()};
-            gmpm_status s = gmpm_scene_create(ctx, &r.desc, &init, &r.scene);
-            r.t_admit = now_s() - t0;
+            gmpm_scene* scene = nullptr;
+            gmpm_status s = gmpm_scene_create(ctx, &r.desc, &init, &scene);
+            const double ta = now_s() - t0;
             if (s != GMPM_OK) {
+                std::lock_guard<std::mutex> lk(mu);
+                r.t_admit = r.t_finish = ta;
                 r.state = GMPM_REQUEST_FAILED;
                 r.status = s;
-                r.t_finish = r.t_admit;
                 ++st.failed;
                 continue;
             }
-            r.bytes = std::max(r.est_bytes, r.scene->impl->device_bytes());
-            used += r.bytes;
-            r.state = GMPM_REQUEST_RUNNING;
             std::vector<double>().swap(r.pos);  // the device holds the state now
             std::vector<double>().swap(r.vel);
             std::vector<double>().swap(r.mass);
             std::vector<int32_t>().swap(r.mat);
-            live.push_back(r.id);
+            r.bytes = std::max(r.est_bytes, scene->impl->device_bytes());
+            live.push_back(&r);
+            batch_stale = true;
+            std::lock_guard<std::mutex> lk(mu);
+            used += r.bytes;
+            r.scene = scene;
+            r.t_admit = ta;
+            r.state = GMPM_REQUEST_RUNNING;
             ++st.admitted;
-            drop_batch();
+            ++st.live;
         }
     }
 
-    gmpm_status retire(Request& r, cudaStream_t s) {
-        r.status = gmpm_scene_sync(r.scene);
-        for (int f : kKeptFields) {
-            std::vector<float>& v = r.results[f];
-            v.resize((size_t)r.n * kept_components(f));
-            gmpm_status e = gmpm_read_particles(r.scene, f, GMPM_DTYPE_F32, GMPM_ORDER_ORIGINAL, v.data(),
-                                                v.size() * sizeof(float), s);
-            if (e != GMPM_OK && r.status == GMPM_OK) r.status = e;
+    // Enqueue the final reads of a request that reached its horizon, then
+    // release its scene on the same stream: nothing here waits for the GPU.
+    gmpm_status retire_begin(Request& r, cudaStream_t s) {
+        const double tr = now_s();
+        size_t need = 64;
+        for (int q = 0; q < 4; ++q) {
+            r.offset[q] = need;
+            need += (size_t)r.n * kept_components(kKeptFields[q]) * sizeof(float);
         }
+        unsigned char* buf = nullptr;
+        size_t got = 0;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            buf = pinned.acquire(need, &got);
+        }
+        gmpm_status e = buf ? GMPM_OK : GMPM_OOM;
+        if (e == GMPM_OK) {
+            r.flags = reinterpret_cast<unsigned int*>(buf);
+            e = r.scene->impl->enqueue_flags(r.flags, s);
+            for (int q = 0; q < 4 && e == GMPM_OK; ++q)
+                e = r.scene->impl->enqueue_read(kKeptFields[q], GMPM_DTYPE_F32, GMPM_ORDER_ORIGINAL, buf + r.offset[q],
+                                                s);
+        }
+        if (!r.ready) {
+            if (!spare_events.empty()) {
+                r.ready = spare_events.back();
+                spare_events.pop_back();
+            } else {
+                cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming);
+            }
+        }
+        cudaEventRecord(r.ready, s);
+        r.scene->impl->set_release_stream(s);  // its last use was on s: free there, no device sync
         gmpm_scene_destroy(r.scene);
-        r.scene = nullptr;
-        used -= std::min(used, r.bytes);
-        r.state = r.status == GMPM_OK ? GMPM_REQUEST_DONE : GMPM_REQUEST_FAILED;
-        r.t_finish = now_s() - t0;
-        if (r.state == GMPM_REQUEST_DONE)
-            ++st.completed;
-        else
-            ++st.failed;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            used -= std::min(used, r.bytes);
+            r.scene = nullptr;
+            r.results = buf;
+            r.results_bytes = got;
+            if (e != GMPM_OK) r.status = e;
+            st.retire_microseconds += (int64_t)((now_s() - tr) * 1e6);
+        }
+        retiring.push_back(&r);
         return GMPM_OK;
+    }
+
+    // Complete retirements whose reads have landed (all of them when wait).
+    void finish_retirements(bool wait) {
+        std::vector<Request*> still;
+        for (Request* r : retiring) {
+            if (wait)
+                cudaEventSynchronize(r->ready);
+            else if (cudaEventQuery(r->ready) != cudaSuccess) {
+                cudaGetLastError();
+                still.push_back(r);
+                continue;
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            if (r->status == GMPM_OK) r->status = flags_status(*r->flags);
+            r->state = r->status == GMPM_OK ? GMPM_REQUEST_DONE : GMPM_REQUEST_FAILED;
+            r->t_finish = now_s() - t0;
+            --st.live;
+            if (r->state == GMPM_REQUEST_DONE)
+                ++st.completed;
+            else
+                ++st.failed;
+            spare_events.push_back(r->ready);
+            r->ready = nullptr;
+        }
+        retiring.swap(still);
     }
 
     gmpm_status ensure_batch() {
@@ -198,7 +325,7 @@ struct Server {
         drop_batch();
         if (live.empty()) return GMPM_OK;
         std::vector<gmpm_scene*> hs;
-        for (int64_t id : live) hs.push_back(reqs[id]->scene);
+        for (Request* r : live) hs.push_back(r->scene);
         gmpm_batch_options o = tuned ? tuned_opt : gmpm_batch_options{};
         if (!tuned) {
             o.autotune = opt.autotune;
@@ -207,6 +334,7 @@ struct Server {
         gmpm_status s = gmpm_batch_create(ctx, hs.data(), (int)hs.size(), &o, &batch);
         if (s != GMPM_OK) return s;
         batch_stale = false;
+        std::lock_guard<std::mutex> lk(mu);
         ++st.batches;
         return GMPM_OK;
     }
@@ -230,38 +358,49 @@ struct Server {
         if (n < 0) return GMPM_INVALID_ARG;
         SERVE_TRY(cudaSetDevice(ctx->device));
         int left = n;
-        admit();
+        finish_retirements(false);
+        if (live.empty()) admit();
         while (left > 0 && !live.empty()) {
             int64_t k = left;
-            for (int64_t id : live) k = std::min(k, reqs[id]->horizon - reqs[id]->done);
+            for (Request* r : live) k = std::min(k, r->horizon - r->done);
             gmpm_status e = ensure_batch();
             if (e != GMPM_OK) return e;
+            const double tl = now_s();
             e = gmpm_batch_substep(batch, (int)k, s);
             if (e != GMPM_OK) return e;
             remember_tuning();
-            for (int64_t id : live) {
-                reqs[id]->done += k;
-                st.particle_substeps += reqs[id]->n * k;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                st.launch_microseconds += (int64_t)((now_s() - tl) * 1e6);
+                for (Request* r : live) {
+                    r->done += k;
+                    st.particle_substeps += r->n * k;
+                }
+                st.substeps += k;
             }
-            st.substeps += k;
             left -= (int)k;
-            bool changed = false;
-            std::vector<int64_t> still;
-            for (int64_t id : live) {
-                Request& r = *reqs[id];
-                if (r.done >= r.horizon) {
-                    retire(r, s);
+            // While the GPU runs these substeps: create the scenes of waiting
+            // requests (host work), then retire finished ones (waits for the GPU).
+            const size_t before = live.size();
+            admit();
+            bool changed = live.size() != before;
+            std::vector<Request*> still;
+            for (Request* r : live) {
+                if (r->done >= r->horizon) {
+                    retire_begin(*r, s);
                     changed = true;
                 } else {
-                    still.push_back(id);
+                    still.push_back(r);
                 }
             }
             if (changed) {
                 live.swap(still);
                 drop_batch();
-                admit();
             }
+            finish_retirements(false);
         }
+        // nothing left to advance: let the last retirements complete
+        if (live.empty()) finish_retirements(true);
         return GMPM_OK;
     }
 };
@@ -311,6 +450,7 @@ gmpm_status gmpm_server_step(gmpm_server* s, int n_substeps, void* stream) {
 
 gmpm_status gmpm_server_poll(gmpm_server* s, int64_t id, gmpm_request_status* out) {
     if (!s || !out) return GMPM_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->impl.mu);
     auto it = s->impl.reqs.find(id);
     if (it == s->impl.reqs.end()) return GMPM_INVALID_ARG;
     const gmpm::Request& r = *it->second;
@@ -328,32 +468,37 @@ gmpm_status gmpm_server_poll(gmpm_server* s, int64_t id, gmpm_request_status* ou
 
 gmpm_status gmpm_server_read(gmpm_server* s, int64_t id, int field, float* dst, size_t bytes) {
     if (!s || !dst) return GMPM_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->impl.mu);
     auto it = s->impl.reqs.find(id);
     if (it == s->impl.reqs.end() || it->second->state != GMPM_REQUEST_DONE) return GMPM_INVALID_ARG;
-    auto f = it->second->results.find(field);
-    if (f == it->second->results.end()) return GMPM_INVALID_ARG;
-    if (bytes < f->second.size() * sizeof(float)) return GMPM_INVALID_ARG;
-    std::memcpy(dst, f->second.data(), f->second.size() * sizeof(float));
-    return GMPM_OK;
+    const gmpm::Request& r = *it->second;
+    for (int q = 0; q < 4; ++q) {
+        if (gmpm::kKeptFields[q] != field) continue;
+        const size_t sz = (size_t)r.n * gmpm::kept_components(field) * sizeof(float);
+        if (bytes < sz || !r.results) return GMPM_INVALID_ARG;
+        std::memcpy(dst, r.results + r.offset[q], sz);
+        return GMPM_OK;
+    }
+    return GMPM_INVALID_ARG;
 }
 
 gmpm_status gmpm_server_release(gmpm_server* s, int64_t id) {
     if (!s) return GMPM_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->impl.mu);
     auto it = s->impl.reqs.find(id);
     if (it == s->impl.reqs.end()) return GMPM_INVALID_ARG;
     if (it->second->state == GMPM_REQUEST_QUEUED || it->second->state == GMPM_REQUEST_RUNNING)
         return GMPM_INVALID_ARG;
+    s->impl.pinned.release(it->second->results, it->second->results_bytes);
     s->impl.reqs.erase(it);
     return GMPM_OK;
 }
 
 gmpm_status gmpm_server_get_stats(gmpm_server* s, gmpm_server_stats* out) {
     if (!s || !out) return GMPM_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->impl.mu);
     *out = s->impl.st;
-    gmpm_batch_info info;
-    if (s->impl.batch && gmpm_batch_get_info(s->impl.batch, &info) == GMPM_OK)
-        out->capture_microseconds += (int64_t)(info.capture_seconds * 1e6);
-    out->live = (int64_t)s->impl.live.size();
+    // live: counted in st under the lock
     out->queued = (int64_t)s->impl.queue.size();
     out->device_bytes_in_use = (int64_t)s->impl.used;
     return GMPM_OK;

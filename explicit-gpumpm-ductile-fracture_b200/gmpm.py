@@ -137,7 +137,8 @@ class RequestStatus(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [(k, C.c_int64) for k in ("submitted", "admitted", "completed", "failed", "live", "queued",
                                           "substeps", "particle_substeps", "batches", "device_bytes_in_use",
-                                          "capture_microseconds")]
+                                          "capture_microseconds", "admit_microseconds", "retire_microseconds",
+                                          "launch_microseconds")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

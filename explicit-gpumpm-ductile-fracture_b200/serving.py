@@ -2,10 +2,10 @@
 gmpm_server (continuous batching), with request latency percentiles and the
 aggregate particle-substeps/s.
 
-Arrivals are generated ahead of time by a background thread (the request's
-particles are part of the request, not of the server's work); the main thread
-submits each request when its arrival time comes, advances the server in
-chunks of substeps, and collects finished requests.
+A producer thread generates each request (its particles are part of the
+request, not of the server's work) and submits it at its arrival time; the
+main thread advances the server in chunks of substeps and collects finished
+requests.  The server accepts submissions while it is being stepped.
 """
 from __future__ import annotations
 
@@ -31,58 +31,80 @@ def run_served(ctx: G.Context, duration_s: float = 600.0, rate_hz: float = 20.0,
         if t > duration_s:
             break
         arrivals.append(t)
-    specs: queue.Queue = queue.Queue(maxsize=64)
+    srv = G.Server(ctx, hbm_budget_bytes=budget_bytes, max_live=max_live)
+    submitted: queue.Queue = queue.Queue()
+    t0 = time.perf_counter()
+    submit_s = [0.0]
 
     def produce():
+        # generates each request ahead of its arrival and submits it on time
+        # (the server accepts submissions while another thread steps it)
         prng = np.random.default_rng(seed + 1)
-        for k in range(len(arrivals)):
-            specs.put(S.served_request(prng, k, lo, hi))
-        specs.put(None)
-
-    threading.Thread(target=produce, daemon=True).start()
-    srv = G.Server(ctx, hbm_budget_bytes=budget_bytes, max_live=max_live)
-    t0 = time.perf_counter()
-    pending = {}  # request id -> (particles, horizon)
-    done = []
-    submitted = 0
-    peak_queue = 0
-    nxt = specs.get()
-    while True:
-        now = time.perf_counter() - t0
-        while nxt is not None and submitted < len(arrivals) and arrivals[submitted] <= now:
-            sp, horizon = nxt
+        for k, t_arr in enumerate(arrivals):
+            sp, horizon = S.served_request(prng, k, lo, hi)
+            wait = t_arr - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            t1 = time.perf_counter()
             rid = srv.submit_spec(sp, horizon)
-            pending[rid] = (sp.n, horizon)
-            submitted += 1
-            nxt = specs.get()
+            submit_s[0] += time.perf_counter() - t1
+            submitted.put(rid)
+        submitted.put(None)
+
+    producer = threading.Thread(target=produce, daemon=True)
+    producer.start()
+    pending = set()
+    done = []
+    n_submitted = 0
+    producer_done = False
+    peak_queue = 0
+    step_s = poll_s = 0.0
+    while True:
+        while True:
+            try:
+                rid = submitted.get_nowait()
+            except queue.Empty:
+                break
+            if rid is None:
+                producer_done = True
+            else:
+                pending.add(rid)
+                n_submitted += 1
+        now = time.perf_counter() - t0
         if now > duration_s + drain_s:
             break
         st = srv.stats()
         peak_queue = max(peak_queue, st["queued"])
         if st["live"] == 0 and st["queued"] == 0:
-            if nxt is None or submitted >= len(arrivals):
+            if producer_done and not pending:
                 break
-            time.sleep(min(0.002, max(0.0, arrivals[submitted] - now)))
+            time.sleep(0.001)
             continue
+        t1 = time.perf_counter()
         srv.step(chunk, stream)
+        t2 = time.perf_counter()
+        step_s += t2 - t1
         for rid in list(pending):
             p = srv.poll(rid)
             if p["state"] in (G.REQUEST_DONE, G.REQUEST_FAILED):
                 done.append(dict(latency=p["finish_time"] - p["submit_time"], queue=p["admit_time"] - p["submit_time"],
                                  n=p["n_particles"], horizon=p["horizon"], ok=p["state"] == G.REQUEST_DONE))
                 srv.release(rid)
-                del pending[rid]
+                pending.discard(rid)
+        poll_s += time.perf_counter() - t2
     elapsed = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
     lat = np.array([d["latency"] for d in done if d["ok"]]) if done else np.zeros(0)
     return dict(
-        duration_s=elapsed, arrivals=len(arrivals), submitted=submitted, completed=int(sum(d["ok"] for d in done)),
+        duration_s=elapsed, arrivals=len(arrivals), submitted=n_submitted, completed=int(sum(d["ok"] for d in done)),
         failed=int(sum(not d["ok"] for d in done)), unfinished=len(pending),
         p50_latency_s=float(np.percentile(lat, 50)) if len(lat) else None,
         p99_latency_s=float(np.percentile(lat, 99)) if len(lat) else None,
         mean_queue_s=float(np.mean([d["queue"] for d in done])) if done else None,
         particle_substeps_per_s=st["particle_substeps"] / elapsed, batches=st["batches"],
-        capture_s=st["capture_microseconds"] / 1e6, max_live=max_live, peak_queue=peak_queue,
+        capture_s=st["capture_microseconds"] / 1e6, admit_s=st["admit_microseconds"] / 1e6,
+        retire_s=st["retire_microseconds"] / 1e6, launch_s=st["launch_microseconds"] / 1e6,
+        step_s=step_s, poll_s=poll_s, submit_s=submit_s[0], max_live=max_live, peak_queue=peak_queue,
         substeps=st["substeps"], rate_hz=rate_hz, sizes=[lo, hi], horizons=[200, 2000],
         budget_bytes=budget_bytes)

@@ -471,6 +471,9 @@ typedef struct gmpm_server_stats {
     int64_t batches;            /* batches built (one per change of the live set) */
     int64_t device_bytes_in_use;
     int64_t capture_microseconds; /* host time spent capturing batch graphs */
+    int64_t admit_microseconds;   /* host time creating admitted scenes */
+    int64_t retire_microseconds;  /* host time retiring scenes (waits for their last substeps, reads results) */
+    int64_t launch_microseconds;  /* host time enqueueing batched substeps */
 } gmpm_server_stats;
 
 void gmpm_server_options_defaults(gmpm_server_options* opt);
