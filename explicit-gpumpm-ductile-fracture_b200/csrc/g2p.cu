@@ -216,22 +216,38 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
             bspline1d_g(xp[0], inv_dx, wx, gx);
             bspline1d_g(xp[1], inv_dx, wy, gy);
             bspline1d_g(xp[2], inv_dx, wz, gz);
+            // Gather of v, dc, grad v, B and grad c over the 3x3x3 stencil
+            // (G2PKernal.cu:286-357, AxG2P_APIC :1085-1112).  The weights are
+            // tensor products w = X_i Y_j Z_k, and the APIC offset x_i - x_p
+            // splits per axis, so the sums are taken one axis at a time: over
+            // k for each (i, j) column, then over j, then over i.
             R vp[3] = {R(0), R(0), R(0)}, dcp = R(0);
             R gv[9], Bn[9], gc[3] = {R(0), R(0), R(0)};
 #pragma unroll
             for (int q = 0; q < 9; ++q) gv[q] = Bn[q] = R(0);
+            R wxd[3], wyd[3], wzd[3];  // weight x (node - particle) offset per axis
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                wxd[q] = wx[q] * (R(q) * dx - xp[0]);
+                wyd[q] = wy[q] * (R(q) * dx - xp[1]);
+                wzd[q] = wz[q] * (R(q) * dx - xp[2]);
+            }
             const R(*win4)[4] = S.win4[u0w];
             const R* wincn = S.wincn[u0w];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                const R d0 = R(i) * dx - xp[0];
+                // sums over j for this i: T0 (Y Z), Ty (Y' Z), Tz (Y Z'), Tdy (Y d Z), Tdz (Y Z d)
+                R T0[3], Ty[3], Tz[3], Tdy[3], Tdz[3], Td = R(0), Tc0 = R(0), Tcy = R(0), Tcz = R(0);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) T0[a] = Ty[a] = Tz[a] = Tdy[a] = Tdz[a] = R(0);
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    const R d1 = R(j) * dx - xp[1];
-                    const R wxy = wx[i] * wy[j], gxy0 = gx[i] * wy[j], gxy1 = wx[i] * gy[j];
+                    // sums over k for column (i, j): Z0 (Z), Z1 (Z'), Z2 (Z d)
+                    R Z0[3], Z1[3], Z2[3], Zd = R(0), C0 = R(0), C1 = R(0);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) Z0[a] = Z1[a] = Z2[a] = R(0);
 #pragma unroll
                     for (int kk = 0; kk < 3; ++kk) {
-                        const R d2 = R(kk) * dx - xp[2];
                         const int node = (li + i) * 36 + (lj + j) * 6 + (lk + kk);
                         R nv[4];
                         if (sizeof(R) == 4) {
@@ -240,27 +256,44 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
                             *reinterpret_cast<double2*>(nv) = *reinterpret_cast<const double2*>(&win4[node][0]);
                             *reinterpret_cast<double2*>(nv + 2) = *reinterpret_cast<const double2*>(&win4[node][2]);
                         }
-                        const R n0 = nv[0], n1 = nv[1], n2 = nv[2], ndc = nv[3], ncn = wincn[node];
-                        const R w = wxy * wz[kk];
-                        const R wg[3] = {gxy0 * wz[kk], gxy1 * wz[kk], wxy * gz[kk]};
-                        vp[0] += w * n0;
-                        vp[1] += w * n1;
-                        vp[2] += w * n2;
-                        dcp += w * ndc;
-                        const R dd[3] = {d0, d1, d2};
+                        const R ncn = wincn[node];
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            gv[0 + 3 * c] += n0 * wg[c];
-                            gv[1 + 3 * c] += n1 * wg[c];
-                            gv[2 + 3 * c] += n2 * wg[c];
-                            const R wd = w * dd[c];
-                            Bn[0 + 3 * c] += n0 * wd;
-                            Bn[1 + 3 * c] += n1 * wd;
-                            Bn[2 + 3 * c] += n2 * wd;
-                            gc[c] += wg[c] * ncn;
+                        for (int a = 0; a < 3; ++a) {
+                            Z0[a] += wz[kk] * nv[a];
+                            Z1[a] += gz[kk] * nv[a];
+                            Z2[a] += wzd[kk] * nv[a];
                         }
+                        Zd += wz[kk] * nv[3];
+                        C0 += wz[kk] * ncn;
+                        C1 += gz[kk] * ncn;
                     }
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        T0[a] += wy[j] * Z0[a];
+                        Ty[a] += gy[j] * Z0[a];
+                        Tz[a] += wy[j] * Z1[a];
+                        Tdy[a] += wyd[j] * Z0[a];
+                        Tdz[a] += wy[j] * Z2[a];
+                    }
+                    Td += wy[j] * Zd;
+                    Tc0 += wy[j] * C0;
+                    Tcy += gy[j] * C0;
+                    Tcz += wy[j] * C1;
                 }
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    vp[a] += wx[i] * T0[a];
+                    gv[a + 0] += gx[i] * T0[a];
+                    gv[a + 3] += wx[i] * Ty[a];
+                    gv[a + 6] += wx[i] * Tz[a];
+                    Bn[a + 0] += wxd[i] * T0[a];
+                    Bn[a + 3] += wx[i] * Tdy[a];
+                    Bn[a + 6] += wx[i] * Tdz[a];
+                }
+                dcp += wx[i] * Td;
+                gc[0] += gx[i] * Tc0;
+                gc[1] += wx[i] * Tcy;
+                gc[2] += wx[i] * Tcz;
             }
             // damage: irreversible (G2PKernal.cu:359-366)
             const R c_old = S.p[buf][P_C][t];
