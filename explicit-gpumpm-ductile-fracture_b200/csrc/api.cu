@@ -288,6 +288,13 @@ struct Scene : SceneBase {
         }
         for (void* p : allocs) cudaFreeAsync(p, rs);
         if (staging) cudaFreeAsync(staging, rs);
+        if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+        for (int b = 0; b < 2; ++b) {
+            if (rstage_[b]) cudaFreeAsync(rstage_[b], rs);
+            if (rstage_packed_[b]) cudaEventDestroy(rstage_packed_[b]);
+            if (rstage_free_[b]) cudaEventDestroy(rstage_free_[b]);
+        }
+        if (copy_stream_) cudaStreamDestroy(copy_stream_);
         if (pcg_done_host) cudaFreeHost(pcg_done_host);
         if (bc_staging) cudaFreeHost(bc_staging);
         if (dt_staging) cudaFreeHost(dt_staging);
@@ -726,6 +733,55 @@ struct Scene : SceneBase {
         return GMPM_OK;
     }
 
+    // Ping-pong device staging for overlapped reads: a read packs on the
+    // caller's stream into the buffer whose previous copy has finished, and
+    // copies to the caller's memory on the copy stream.
+    cudaStream_t copy_stream_ = nullptr;
+    void* rstage_[2] = {nullptr, nullptr};
+    size_t rstage_bytes_[2] = {0, 0};
+    cudaEvent_t rstage_packed_[2] = {nullptr, nullptr}, rstage_free_[2] = {nullptr, nullptr};
+    int rnext_ = 0;
+
+    gmpm_status read_particles_async(int field, int dtype, int order, void* dst, size_t bytes,
+                                     cudaStream_t s) override {
+        const int nc = field_components(field);
+        if (nc == 0 || !dst) return GMPM_INVALID_ARG;
+        if (dtype < 0 || dtype > 2 || order < 0 || order > 1) return GMPM_INVALID_ARG;
+        const size_t need = (size_t)n * nc * (dtype == GMPM_DTYPE_F64 ? 8 : 4);
+        if (bytes < need) return GMPM_INVALID_ARG;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        if (!copy_stream_) {
+            GMPM_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+            for (int b = 0; b < 2; ++b) {
+                GMPM_TRY(cudaEventCreateWithFlags(&rstage_packed_[b], cudaEventDisableTiming));
+                GMPM_TRY(cudaEventCreateWithFlags(&rstage_free_[b], cudaEventDisableTiming));
+                GMPM_TRY(cudaEventRecord(rstage_free_[b], copy_stream_));
+            }
+        }
+        const int b = rnext_;
+        rnext_ ^= 1;
+        GMPM_TRY(cudaStreamWaitEvent(s, rstage_free_[b], 0));  // the buffer's previous copy has left
+        if (rstage_bytes_[b] < need) {
+            if (rstage_[b]) cudaFreeAsync(rstage_[b], s);
+            rstage_[b] = nullptr;
+            rstage_bytes_[b] = 0;
+            GMPM_TRY(cudaMallocAsync(&rstage_[b], need, s));
+            rstage_bytes_[b] = need;
+        }
+        GMPM_TRY(launch_pack_field<R>(st[cur], aux, field, dtype, order, n, rstage_[b], s));
+        GMPM_TRY(cudaEventRecord(rstage_packed_[b], s));
+        GMPM_TRY(cudaStreamWaitEvent(copy_stream_, rstage_packed_[b], 0));
+        GMPM_TRY(cudaMemcpyAsync(dst, rstage_[b], need, cudaMemcpyDefault, copy_stream_));
+        GMPM_TRY(cudaEventRecord(rstage_free_[b], copy_stream_));
+        return GMPM_OK;
+    }
+
+    gmpm_status reads_wait() override {
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        if (copy_stream_) GMPM_TRY(cudaStreamSynchronize(copy_stream_));
+        return GMPM_OK;
+    }
+
     gmpm_status read_binning(int array, void* dst, size_t bytes) override {
         if (!dst) return GMPM_INVALID_ARG;
         GMPM_TRY(cudaSetDevice(ctx->device));
@@ -1141,6 +1197,17 @@ gmpm_status gmpm_read_particles(gmpm_scene* s, int field, int dtype, int order, 
                                 void* stream) {
     if (!s) return GMPM_INVALID_ARG;
     return s->impl->read_particles(field, dtype, order, dst, bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+gmpm_status gmpm_read_particles_async(gmpm_scene* s, int field, int dtype, int order, void* dst, size_t bytes,
+                                      void* stream) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->read_particles_async(field, dtype, order, dst, bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+gmpm_status gmpm_read_wait(gmpm_scene* s) {
+    if (!s) return GMPM_INVALID_ARG;
+    return s->impl->reads_wait();
 }
 
 gmpm_status gmpm_set_dt(gmpm_scene* s, double dt, void* stream) {

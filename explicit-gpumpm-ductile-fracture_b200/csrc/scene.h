@@ -23,6 +23,11 @@ struct SceneBase {
     virtual gmpm_status substep_timed(int n, cudaStream_t s, gmpm_stage_times* out) = 0;
     virtual gmpm_status rebin(cudaStream_t s) = 0;
     virtual gmpm_status read_particles(int field, int dtype, int order, void* dst, size_t bytes, cudaStream_t s) = 0;
+    // Read overlapped with later work: packed on s, copied on the scene's copy
+    // stream; complete after reads_wait.
+    virtual gmpm_status read_particles_async(int field, int dtype, int order, void* dst, size_t bytes,
+                                             cudaStream_t s) = 0;
+    virtual gmpm_status reads_wait() = 0;
     virtual gmpm_status read_binning(int array, void* dst, size_t bytes) = 0;
     virtual gmpm_status diagnostics(gmpm_diag* out) = 0;
     virtual gmpm_status sync() = 0;

@@ -163,6 +163,9 @@ SIGNATURES = {
     "gmpm_scene_sync": (C.c_int, [C.c_void_p]),
     "gmpm_read_particles": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
     "gmpm_read_binning": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    "gmpm_read_particles_async": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t,
+                                            C.c_void_p]),
+    "gmpm_read_wait": (C.c_int, [C.c_void_p]),
     "gmpm_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Diag)]),
     "gmpm_status_string": (C.c_char_p, [C.c_int]),
     "gmpm_bin_positions_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_int, C.c_int, C.c_int,
@@ -351,6 +354,15 @@ class Scene:
                   dtype: int = DTYPE_F32, stream: int | None = None) -> None:
         check(lib().gmpm_read_particles(self.h, FIELD[field], dtype, order, C.c_void_p(out_ptr), nbytes,
                                         C.c_void_p(stream) if stream else None), f"read_particles({field})")
+
+    def read_into_async(self, field: str, out_ptr: int, nbytes: int, order: int = ORDER_INTERNAL,
+                        dtype: int = DTYPE_F32, stream: int | None = None) -> None:
+        """Overlapped read into (pinned) host memory; complete after read_wait()."""
+        check(lib().gmpm_read_particles_async(self.h, FIELD[field], dtype, order, C.c_void_p(out_ptr), nbytes,
+                                              C.c_void_p(stream) if stream else None), f"read_particles_async({field})")
+
+    def read_wait(self) -> None:
+        check(lib().gmpm_read_wait(self.h), "read_wait")
 
     def binning(self, array: str) -> np.ndarray:
         counts = np.zeros(4, dtype=np.int64)

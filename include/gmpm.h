@@ -306,6 +306,16 @@ gmpm_status gmpm_read_particles(gmpm_scene* scene, int field, int dtype, int ord
  * the reference keeps in Particles/DomainTransformer device members
  * (d_indexTrans, cell_id, d_page2particle, d_cell2particle, d_adjPage:
  * GPU_MPM/Particles.cuh:26-44, Transformer.cuh:35-50). */
+/* Overlapped read for frame loops (Attribs_Back_Host, Particles.cpp:33-52, without the stall): the
+ * field is packed on `stream` after the work already queued there and copied to dst on the scene's
+ * own copy stream, so later substeps on `stream` run while it travels.  dst must stay valid, and
+ * should be pinned host memory, until gmpm_read_wait returns.  Two reads may be in flight; a third
+ * waits on the device for the oldest. */
+gmpm_status gmpm_read_particles_async(gmpm_scene* scene, int field, int dtype, int order, void* dst, size_t bytes,
+                                      void* stream);
+/* Wait until every overlapped read of the scene has landed. */
+gmpm_status gmpm_read_wait(gmpm_scene* scene);
+
 gmpm_status gmpm_read_binning(gmpm_scene* scene, int array, void* dst, size_t bytes);
 
 /* Conservation / CFL diagnostics computed on the device in FP64.  Replaces

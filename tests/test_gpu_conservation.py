@@ -96,3 +96,31 @@ def test_table_capacity_overflow(pkg, ctx):
     with pytest.raises(G.GmpmError) as e:
         sp.build(ctx)
     assert e.value.status == G.TABLE_OVERFLOW
+
+
+def test_overlapped_reads_match_blocking_reads(pkg, ctx):
+    """gmpm_read_particles_async: reads queued behind later substeps (more than
+    the two staging buffers in flight) land as the blocking reads of the same
+    substeps."""
+    import torch
+
+    G = pkg.gmpm
+    sp = pkg.scenes.notched_bar()
+    a, b = sp.build(ctx), sp.build(ctx)
+    want, got = [], []
+    for _ in range(4):
+        a.substep(1)
+        want.append((a.read("position", order=G.ORDER_INTERNAL, dtype=G.DTYPE_F32),
+                     a.read("damage", order=G.ORDER_INTERNAL, dtype=G.DTYPE_F32)))
+        pos = torch.empty(sp.n * 3, dtype=torch.float32, pin_memory=True)
+        dmg = np.empty(sp.n, dtype=np.float32)  # pageable destinations are allowed too
+        b.substep(1)
+        b.read_into_async("position", pos.data_ptr(), pos.numel() * 4)
+        b.read_into_async("damage", dmg.ctypes.data, dmg.nbytes)
+        got.append((pos, dmg))
+    b.read_wait()
+    for (wp, wd), (gp, gd) in zip(want, got):
+        assert np.array_equal(wp.reshape(-1), gp.numpy()), "position"
+        assert np.array_equal(wd.reshape(-1), gd), "damage"
+    with pytest.raises(G.GmpmError):
+        b.read_into_async("position", 0, sp.n * 12)
