@@ -144,18 +144,24 @@ __global__ void k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys, cons
     keys_sorted[slot] = key;
 }
 
-// Canonical in-cell order: ascending previous slot.  One CTA per page; the
-// page's slots are ranked in shared memory (cells hold few particles).  A page
-// above the buffer is done in windows of whole cells; a single cell above the
-// buffer (thousands of particles in one cell, which only a failed state with
-// clamped positions produces) keeps its scatter order and raises
-// GMPM_FLAG_TABLE_OVERFLOW instead of being ranked in quadratic time.
-constexpr int kCanonBuf = 4096;
+// Canonical in-cell order: ascending previous slot.  Each warp takes one page
+// (8 pages per CTA in flight, so the page's few dependent global round trips
+// overlap across pages) and ranks every slot within its cell in shared memory
+// (cells hold few particles).  A page above the warp's buffer is left to the
+// whole CTA, which ranks it in windows of whole cells after the warps'
+// pages; a single cell above the CTA buffer (thousands of particles in one
+// cell, which only a failed state with clamped positions produces) keeps its
+// scatter order and raises GMPM_FLAG_TABLE_OVERFLOW instead of being ranked
+// in quadratic time.
+constexpr int kCanonWarps = 8;
+constexpr int kCanonWarpBuf = 768;
+constexpr int kCanonBuf = kCanonWarps * kCanonWarpBuf;
 
-__device__ __forceinline__ void canon_window(const BinDev& bin, const int32_t* cs, int32_t* buf, int lo, int hi) {
-    for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) buf[s - lo] = bin.perm[s];
-    __syncthreads();
-    for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+// Rank slots [lo, hi) of a page (whole cells) by previous slot within their
+// cells; buf holds perm[lo, hi).  Threads tid, tid + step, ... of the caller.
+__device__ __forceinline__ void canon_rank(const BinDev& bin, const int32_t* cs, const int32_t* buf, int lo, int hi,
+                                           int tid, int step) {
+    for (int s = lo + tid; s < hi; s += step) {
         const int cell = (int)(bin.keys_sorted[s] & 63);
         const int a = cs[cell] - lo, e = cs[cell + 1] - lo;
         const int32_t v = buf[s - lo];
@@ -163,33 +169,54 @@ __device__ __forceinline__ void canon_window(const BinDev& bin, const int32_t* c
         for (int u = a; u < e; ++u) r += buf[u] < v;
         bin.perm[lo + a + r] = v;
     }
-    __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_bin_canon(BinDev bin, Counters* cnt) {
+__global__ void __launch_bounds__(32 * kCanonWarps) k_bin_canon(BinDev bin, Counters* cnt) {
     __shared__ int32_t buf[kCanonBuf];
-    __shared__ int32_t cs[65];
+    __shared__ int32_t cs[kCanonWarps][68];
+    __shared__ int big[kCanonWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nb = min(cnt->n_blocks, bin.nb_cap);
-    for (int b = blockIdx.x; b < nb; b += gridDim.x) {
-        __syncthreads();
-        for (int q = threadIdx.x; q < 65; q += blockDim.x) cs[q] = bin.cell_start[(int64_t)b * 64 + q];
-        __syncthreads();
-        if (cs[64] - cs[0] <= kCanonBuf) {
-            canon_window(bin, cs, buf, cs[0], cs[64]);
-            continue;
-        }
-        int c0 = 0;
-        while (c0 < 64) {
-            int c1 = c0;
-            while (c1 < 64 && cs[c1 + 1] - cs[c0] <= kCanonBuf) ++c1;
-            if (c1 == c0) {
-                if (threadIdx.x == 0) raise_flag(cnt, GMPM_FLAG_TABLE_OVERFLOW);
-                c0 = c0 + 1;
-                continue;
+    int32_t* wbuf = buf + warp * kCanonWarpBuf;
+    for (int g = blockIdx.x * kCanonWarps; g < nb; g += gridDim.x * kCanonWarps) {
+        const int b = g + warp;
+        int is_big = 0;
+        if (b < nb) {
+            for (int q = lane; q < 65; q += 32) cs[warp][q] = bin.cell_start[(int64_t)b * 64 + q];
+            __syncwarp();
+            const int lo = cs[warp][0], hi = cs[warp][64];
+            if (hi - lo <= kCanonWarpBuf) {
+                for (int s = lo + lane; s < hi; s += 32) wbuf[s - lo] = bin.perm[s];
+                __syncwarp();
+                canon_rank(bin, cs[warp], wbuf, lo, hi, lane, 32);
+            } else {
+                is_big = 1;
             }
-            canon_window(bin, cs, buf, cs[c0], cs[c1]);
-            c0 = c1;
         }
+        if (lane == 0) big[warp] = is_big;
+        __syncthreads();
+        // pages above a warp's buffer: the whole CTA, one at a time
+        for (int w = 0; w < kCanonWarps; ++w) {
+            if (!big[w]) continue;
+            const int32_t* pcs = cs[w];
+            int c0 = 0;
+            while (c0 < 64) {
+                int c1 = c0;
+                while (c1 < 64 && pcs[c1 + 1] - pcs[c0] <= kCanonBuf) ++c1;
+                if (c1 == c0) {
+                    if (threadIdx.x == 0) raise_flag(cnt, GMPM_FLAG_TABLE_OVERFLOW);
+                    c0 = c0 + 1;
+                    continue;
+                }
+                const int lo = pcs[c0], hi = pcs[c1];
+                for (int s = lo + (int)threadIdx.x; s < hi; s += blockDim.x) buf[s - lo] = bin.perm[s];
+                __syncthreads();
+                canon_rank(bin, pcs, buf, lo, hi, threadIdx.x, blockDim.x);
+                __syncthreads();
+                c0 = c1;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -219,7 +246,7 @@ cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bi
     cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), stream);
     k_bin_scatter<<<gn, T, 0, stream>>>(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, bin.perm,
                                         bin.keys_sorted, bin.nb_cap);
-    k_bin_canon<<<num_sms * 4, 256, 0, stream>>>(bin, cnt);
+    k_bin_canon<<<num_sms * 8, 32 * kCanonWarps, 0, stream>>>(bin, cnt);
     return cudaGetLastError();
 }
 

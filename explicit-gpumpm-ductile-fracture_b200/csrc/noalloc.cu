@@ -159,7 +159,7 @@ extern "C" gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    k_bin_canon<<<sms * 4, 256, 0, s>>>(bin, cnt);
+    k_bin_canon<<<sms * 8, 256, 0, s>>>(bin, cnt);  // 8 warps, one page each
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? GMPM_OOM : GMPM_CUDA_ERROR;
     return GMPM_OK;

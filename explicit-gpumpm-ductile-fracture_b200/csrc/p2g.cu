@@ -353,7 +353,11 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
     const int g = le / 9;
     const int col = le - g * 9;
     const int ci = col / 3, cj = col - ci * 3;
-    const int cb = (warp >> 2) * 16 + (warp & 3) * 4;  // first cell (cz = 0) of the z-column
+    // Warp w owns z-column (cx, cy) = (w / 4, (w - cx) mod 4): the four warps
+    // of a scheduler (w mod 4) then hold one column of every cx and every cy,
+    // so a page's empty rows or slabs of cells do not all land on one scheduler.
+    const int wcx = warp >> 2, wcy = ((warp & 3) - wcx) & 3;
+    const int cb = wcx * 16 + wcy * 4;  // first cell (cz = 0) of the z-column
     const R inv_dx = sc->inv_dx;
     const R fi = R(ci), fj = R(cj);
     Piece<R> px, py;
@@ -454,7 +458,7 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
         // record buffer, which is free once every warp is past its sweep.
         __syncthreads();
         R* acc_smem = recs;
-        const int a = (warp >> 2) + ci, bb = (warp & 3) + cj;
+        const int a = wcx + ci, bb = wcy + cj;
         if (!kDeterministic) {
             for (int q = t; q < kP2GChannels * kWindowNodes; q += kP2GThreads) acc_smem[q] = R(0);
             __syncthreads();
@@ -466,7 +470,7 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
 #pragma unroll
                 for (int z = 0; z < 6; ++z) {
                     if (kDeterministic)
-                        acc_smem[(warp * 9 + col) * kColAcc + z * 9 + ch] = acc[3 * z + q];
+                        acc_smem[((wcx * 4 + wcy) * 9 + col) * kColAcc + z * 9 + ch] = acc[3 * z + q];
                     else
                         atomicAdd(&acc_smem[ch * kWindowNodes + a * 36 + bb * 6 + z], acc[3 * z + q]);
                 }
