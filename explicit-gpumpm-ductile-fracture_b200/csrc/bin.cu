@@ -9,6 +9,7 @@
 // Particles are counting-sorted by (page rank, cell); the in-cell order is
 // then made canonical (ascending previous slot), so the result equals a
 // stable sort by (key, previous slot) bit for bit.  No host synchronisation.
+#include <algorithm>
 #include <cstdint>
 
 #include "kernels.h"
@@ -16,37 +17,60 @@
 
 namespace gmpm {
 
+// Particles per thread of the streaming binning kernels: each thread takes
+// kBinILP particles one CTA width apart (coalesced per round) and issues all
+// their loads before using any, so more requests are in flight per SM.
+constexpr int kBinThreads = 256;
+constexpr int kBinILP = 4;
+
 template <typename R>
-__global__ void k_bin_keys(int64_t n, const R* __restrict__ x0, const R* __restrict__ x1, const R* __restrict__ x2,
-                           const SceneDev<R>* __restrict__ sc, uint32_t* __restrict__ keys,
-                           uint8_t* __restrict__ page_flag, Counters* cnt) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(kBinThreads) k_bin_keys(int64_t n, const R* __restrict__ x0,
+                                                          const R* __restrict__ x1, const R* __restrict__ x2,
+                                                          const SceneDev<R>* __restrict__ sc,
+                                                          uint32_t* __restrict__ keys,
+                                                          uint8_t* __restrict__ page_flag, Counters* cnt) {
+    const int64_t i0 = (int64_t)blockIdx.x * kBinThreads * kBinILP + threadIdx.x;
     const double inv_dx = sc->inv_dx_d;
-    const double xs[3] = {(double)x0[i], (double)x1[i], (double)x2[i]};
-    int base[3];
-    bool bad = false;
+    int hi[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        // (int)(x / dx + 0.5) - 1 as in cal_cellId (Particle_kernal.cu:162-164),
-        // valid when the 3-node stencil stays inside the grid.
-        const double t = __dadd_rn(__dmul_rn(xs[a], inv_dx), 0.5);
-        const int hi = sc->res[a] - 3;
-        if (!(t >= 1.0)) {
-            base[a] = 0;
-            bad = true;
-        } else if (t >= (double)(hi + 2)) {
-            base[a] = hi;
-            bad = true;
-        } else {
-            base[a] = (int)t - 1;
+    for (int a = 0; a < 3; ++a) hi[a] = sc->res[a] - 3;
+    R xs[kBinILP][3];
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u) {
+        const int64_t i = i0 + (int64_t)u * kBinThreads;
+        if (i < n) {
+            xs[u][0] = x0[i];
+            xs[u][1] = x1[i];
+            xs[u][2] = x2[i];
         }
     }
+    bool bad = false;
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u) {
+        const int64_t i = i0 + (int64_t)u * kBinThreads;
+        if (i >= n) continue;
+        int base[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            // (int)(x / dx + 0.5) - 1 as in cal_cellId (Particle_kernal.cu:162-164),
+            // valid when the 3-node stencil stays inside the grid.
+            const double t = __dadd_rn(__dmul_rn((double)xs[u][a], inv_dx), 0.5);
+            if (!(t >= 1.0)) {
+                base[a] = 0;
+                bad = true;
+            } else if (t >= (double)(hi[a] + 2)) {
+                base[a] = hi[a];
+                bad = true;
+            } else {
+                base[a] = (int)t - 1;
+            }
+        }
+        const uint32_t cell = (uint32_t)(((base[0] & 3) << 4) | ((base[1] & 3) << 2) | (base[2] & 3));
+        const uint32_t pk = page_key(base[0] >> 2, base[1] >> 2, base[2] >> 2);
+        keys[i] = (pk << 6) | cell;
+        page_flag[pk] = 1;
+    }
     if (bad) raise_flag(cnt, GMPM_FLAG_OUT_OF_DOMAIN);
-    const uint32_t cell = (uint32_t)(((base[0] & 3) << 4) | ((base[1] & 3) << 2) | (base[2] & 3));
-    const uint32_t pk = page_key(base[0] >> 2, base[1] >> 2, base[2] >> 2);
-    keys[i] = (pk << 6) | cell;
-    page_flag[pk] = 1;
 }
 
 // Mark every active page and its 7 "+" neighbours as grid pages
@@ -103,45 +127,58 @@ __global__ void k_page_links(BinDev bin, const Counters* cnt) {
 }
 
 // Histogram of (page rank, cell) buckets with warp-aggregated atomics.
-__global__ void k_bin_hist(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
-                           int32_t* __restrict__ cell_count, int nb_cap) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < n;
-    int bucket = -1;
-    if (live) {
-        const uint32_t key = keys[i];
-        const int r = page_rank[key >> 6];
-        if (r < nb_cap) bucket = r * 64 + (int)(key & 63);
-    }
-    const unsigned peers = __match_any_sync(0xffffffffu, bucket);
+__global__ void __launch_bounds__(kBinThreads) k_bin_hist(int64_t n, const uint32_t* __restrict__ keys,
+                                                          const int32_t* __restrict__ page_rank,
+                                                          int32_t* __restrict__ cell_count, int nb_cap) {
+    const int64_t i0 = (int64_t)blockIdx.x * kBinThreads * kBinILP + threadIdx.x;
+    uint32_t key[kBinILP];
+    int rank[kBinILP];
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u) key[u] = i0 + (int64_t)u * kBinThreads < n ? keys[i0 + (int64_t)u * kBinThreads] : 0u;
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u)
+        rank[u] = i0 + (int64_t)u * kBinThreads < n ? page_rank[key[u] >> 6] : nb_cap;
     const int lane = threadIdx.x & 31;
-    if (bucket >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cell_count[bucket], __popc(peers));
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u) {
+        const int bucket = rank[u] < nb_cap ? rank[u] * 64 + (int)(key[u] & 63) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, bucket);
+        if (bucket >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cell_count[bucket], __popc(peers));
+    }
 }
 
 // Scatter slots; lanes of one warp with the same bucket keep their order.
-__global__ void k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
-                              const int32_t* __restrict__ cell_start, int32_t* __restrict__ fill,
-                              int32_t* __restrict__ perm, uint32_t* __restrict__ keys_sorted, int nb_cap) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < n;
-    int bucket = -1;
-    uint32_t key = 0;
-    if (live) {
-        key = keys[i];
-        const int r = page_rank[key >> 6];
-        if (r < nb_cap) bucket = r * 64 + (int)(key & 63);
+__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys,
+                                                             const int32_t* __restrict__ page_rank,
+                                                             const int32_t* __restrict__ cell_start,
+                                                             int32_t* __restrict__ fill, int32_t* __restrict__ perm,
+                                                             uint32_t* __restrict__ keys_sorted, int nb_cap) {
+    const int64_t i0 = (int64_t)blockIdx.x * kBinThreads * kBinILP + threadIdx.x;
+    uint32_t key[kBinILP];
+    int bucket[kBinILP], start[kBinILP];
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u) key[u] = i0 + (int64_t)u * kBinThreads < n ? keys[i0 + (int64_t)u * kBinThreads] : 0u;
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u) {
+        const int r = i0 + (int64_t)u * kBinThreads < n ? page_rank[key[u] >> 6] : nb_cap;
+        bucket[u] = r < nb_cap ? r * 64 + (int)(key[u] & 63) : -1;
     }
-    const unsigned peers = __match_any_sync(0xffffffffu, bucket);
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u) start[u] = bucket[u] >= 0 ? cell_start[bucket[u]] : 0;
     const int lane = threadIdx.x & 31;
-    const int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (bucket >= 0 && lane == leader) base = atomicAdd(&fill[bucket], __popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (bucket < 0) return;
-    const int rank = __popc(peers & ((1u << lane) - 1u));
-    const int slot = cell_start[bucket] + base + rank;
-    perm[slot] = (int32_t)i;
-    keys_sorted[slot] = key;
+#pragma unroll
+    for (int u = 0; u < kBinILP; ++u) {
+        const unsigned peers = __match_any_sync(0xffffffffu, bucket[u]);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (bucket[u] >= 0 && lane == leader) base = atomicAdd(&fill[bucket[u]], __popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (bucket[u] >= 0) {
+            const int slot = start[u] + base + __popc(peers & ((1u << lane) - 1u));
+            perm[slot] = (int32_t)(i0 + (int64_t)u * kBinThreads);
+            keys_sorted[slot] = key[u];
+        }
+    }
 }
 
 // Canonical in-cell order: ascending previous slot.  Each warp takes one page
@@ -222,16 +259,37 @@ __global__ void __launch_bounds__(32 * kCanonWarps) k_bin_canon(BinDev bin, Coun
 
 // ---------------------------------------------------------------------------
 
+static unsigned bin_grid(int64_t n) {
+    return (unsigned)std::max<int64_t>(1, (n + (int64_t)kBinThreads * kBinILP - 1) / ((int64_t)kBinThreads * kBinILP));
+}
+
+cudaError_t launch_bin_hist(int64_t n, const uint32_t* keys, const int32_t* page_rank, int32_t* cell_count, int nb_cap,
+                            cudaStream_t s) {
+    k_bin_hist<<<bin_grid(n), kBinThreads, 0, s>>>(n, keys, page_rank, cell_count, nb_cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_scatter(int64_t n, const uint32_t* keys, const int32_t* page_rank, const int32_t* cell_start,
+                               int32_t* fill, int32_t* perm, uint32_t* keys_sorted, int nb_cap, cudaStream_t s) {
+    k_bin_scatter<<<bin_grid(n), kBinThreads, 0, s>>>(n, keys, page_rank, cell_start, fill, perm, keys_sorted, nb_cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_canon(BinDev bin, Counters* cnt, int num_sms, cudaStream_t s) {
+    k_bin_canon<<<num_sms * 8, 32 * kCanonWarps, 0, s>>>(bin, cnt);
+    return cudaGetLastError();
+}
+
 template <typename R>
 cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bin, ScanScratch scan, Counters* cnt,
                            int num_sms, cudaStream_t stream) {
     const int64_t n = bin.n;
     const int T = 256;
-    const unsigned gn = (unsigned)((n + T - 1) / T);
+    const unsigned gn = bin_grid(n);
     const unsigned gk = (bin.key_space + T - 1) / T;
     cudaMemsetAsync(bin.page_flag, 0, bin.key_space, stream);
     cudaMemsetAsync(bin.grid_flag, 0, bin.key_space, stream);
-    k_bin_keys<R><<<gn, T, 0, stream>>>(n, st.x[0], st.x[1], st.x[2], sc, bin.keys, bin.page_flag, cnt);
+    k_bin_keys<R><<<gn, kBinThreads, 0, stream>>>(n, st.x[0], st.x[1], st.x[2], sc, bin.keys, bin.page_flag, cnt);
     scan_exclusive<uint8_t>(bin.page_flag, bin.page_rank, (int64_t)bin.key_space, &cnt->n_blocks, scan, stream);
     k_mark_grid<<<gk, T, 0, stream>>>(bin.key_space, bin.page_flag, bin.grid_flag);
     scan_exclusive<uint8_t>(bin.grid_flag, bin.grid_rank, (int64_t)bin.key_space, &cnt->n_grid_blocks, scan, stream);
@@ -241,19 +299,19 @@ cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bi
     k_page_links<<<(links + T - 1) / T, T, 0, stream>>>(bin, cnt);
     const int64_t ncell = (int64_t)bin.nb_cap * 64;
     cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), stream);
-    k_bin_hist<<<gn, T, 0, stream>>>(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap);
+    launch_bin_hist(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap, stream);
     scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, ncell, bin.cell_start + ncell, scan, stream);
     cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), stream);
-    k_bin_scatter<<<gn, T, 0, stream>>>(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, bin.perm,
-                                        bin.keys_sorted, bin.nb_cap);
-    k_bin_canon<<<num_sms * 8, 32 * kCanonWarps, 0, stream>>>(bin, cnt);
+    launch_bin_scatter(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, bin.perm, bin.keys_sorted,
+                       bin.nb_cap, stream);
+    launch_bin_canon(bin, cnt, num_sms, stream);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t launch_keys(const SceneDev<R>* sc, const PState<R>& st, BinDev bin, Counters* cnt, cudaStream_t s) {
     const int T = 256;
-    k_bin_keys<R><<<(unsigned)((bin.n + T - 1) / T), T, 0, s>>>(bin.n, st.x[0], st.x[1], st.x[2], sc, bin.keys,
+    k_bin_keys<R><<<bin_grid(bin.n), kBinThreads, 0, s>>>(bin.n, st.x[0], st.x[1], st.x[2], sc, bin.keys,
                                                                  bin.page_flag, cnt);
     return cudaGetLastError();
 }

@@ -58,6 +58,12 @@ cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bi
 template <typename R>
 cudaError_t launch_keys(const SceneDev<R>* sc, const PState<R>& st, BinDev bin, Counters* cnt, cudaStream_t s);
 cudaError_t launch_mark_grid(BinDev bin, cudaStream_t s);
+// The counting-sort passes of the binning (also used by the allocation-free entry point).
+cudaError_t launch_bin_hist(int64_t n, const uint32_t* keys, const int32_t* page_rank, int32_t* cell_count, int nb_cap,
+                            cudaStream_t s);
+cudaError_t launch_bin_scatter(int64_t n, const uint32_t* keys, const int32_t* page_rank, const int32_t* cell_start,
+                               int32_t* fill, int32_t* perm, uint32_t* keys_sorted, int nb_cap, cudaStream_t s);
+cudaError_t launch_bin_canon(BinDev bin, Counters* cnt, int num_sms, cudaStream_t s);
 
 // Number of components of a gmpm_field (0 if unknown).
 int field_components(int field);

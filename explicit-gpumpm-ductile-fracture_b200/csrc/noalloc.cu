@@ -45,15 +45,9 @@ static_assert(kNoAllocScratchBytes == GMPM_NOALLOC_SCRATCH_BYTES, "keep include/
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Kernels of bin.cu reused unchanged.
+// Kernel of bin.cu reused unchanged (the counting-sort passes go through the launchers of kernels.h).
 __global__ void k_compact_keys(uint32_t key_space, const uint8_t* __restrict__ flag, const int32_t* __restrict__ rank,
                                uint32_t* __restrict__ out, int cap, Counters* cnt);
-__global__ void k_bin_hist(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
-                           int32_t* __restrict__ cell_count, int nb_cap);
-__global__ void k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys, const int32_t* __restrict__ page_rank,
-                              const int32_t* __restrict__ cell_start, int32_t* __restrict__ fill,
-                              int32_t* __restrict__ perm, uint32_t* __restrict__ keys_sorted, int nb_cap);
-__global__ void k_bin_canon(BinDev bin, Counters* cnt);
 
 // Page/cell keys of interleaved xyz positions: the same FP64 arithmetic as
 // the scene binning (cal_cellId, Particle_kernal.cu:158-165).
@@ -151,15 +145,14 @@ extern "C" gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_
     k_noalloc_keys<<<gn, T, 0, s>>>(n, positions, 1.0 / dx, res_x, res_y, res_z, bin.keys, bin.page_flag, cnt);
     scan_exclusive<uint8_t>(bin.page_flag, bin.page_rank, (int64_t)kNoAllocKeySpace, &cnt->n_blocks, scan, s);
     k_compact_keys<<<gk, T, 0, s>>>(kNoAllocKeySpace, bin.page_flag, bin.page_rank, bin.block_keys, bin.nb_cap, cnt);
-    k_bin_hist<<<gn, T, 0, s>>>(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap);
+    launch_bin_hist(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap, s);
     scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, kNoAllocCells, bin.cell_start + kNoAllocCells, scan, s);
     cudaMemsetAsync(bin.cell_count, 0, kNoAllocCells * sizeof(int32_t), s);
-    k_bin_scatter<<<gn, T, 0, s>>>(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, perm, keys_sorted,
-                                   bin.nb_cap);
+    launch_bin_scatter(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, perm, keys_sorted, bin.nb_cap, s);
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    k_bin_canon<<<sms * 8, 256, 0, s>>>(bin, cnt);  // 8 warps, one page each
+    launch_bin_canon(bin, cnt, sms, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? GMPM_OOM : GMPM_CUDA_ERROR;
     return GMPM_OK;
