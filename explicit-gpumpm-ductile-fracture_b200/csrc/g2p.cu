@@ -3,14 +3,16 @@
 // substep (applyVonMises, ExplicitTimeIntegrator.cu:132-370) and with the
 // phase-field gradient gather (AxG2P_APIC, G2PKernal.cu:1006-1123).
 //
-// Each CTA walks particle pages in runs of up to 256 sorted slots.  For every
-// page it stages the 6x6x6 window of v, dc and c_new in shared memory; one
-// thread per particle then gathers its 3x3x3 stencil, updates c
+// Each CTA takes an equal share of the sorted slots and walks it in units of
+// up to 256 slots that run across page boundaries.  For every page it stages
+// the 6x6x6 window of v, dc and c_new in shared memory; one thread per
+// particle then gathers its 3x3x3 stencil, updates c
 // (irreversibly), x, F = (I + dt grad v) F, the APIC matrix B, runs the SVD +
 // Hencky return map + damage driving force, and writes the particle in the
 // new sorted order.  Reading the previous order through perm and writing the
 // new order is the reorder the reference does with gathers and D2D copies
 // (Particle_kernal.cu:544-573, TimeIntegrator.cu:459-461).
+#include <algorithm>
 #include <cstdint>
 
 #include "async_copy.cuh"
@@ -19,29 +21,40 @@
 
 namespace gmpm {
 
-// Work unit: up to kG2PUnit consecutive sorted slots of one page.  A CTA
-// walks its pages (grid-stride) unit by unit with a three-deep software
-// pipeline of asynchronous copies:
-//   unit k+2: perm, sorted keys, the page's adjacency row and key   (meta)
-//   unit k+1: the particles' 17 input words (through perm) and, when the
-//             unit starts a new page, the page's 6x6x6 node window   (data)
+// Work unit: up to kG2PUnit consecutive sorted slots of the CTA's share,
+// spanning at most kUnitPages pages, so that no thread slot idles at a page
+// end (a page of 385 particles no longer costs a unit of 256 and one of 129).
+// A CTA walks its units with a three-deep software pipeline of asynchronous
+// copies:
+//   unit k+2: perm, sorted keys, and its pages' adjacency rows and keys  (meta)
+//   unit k+1: the particles' 17 input words (through perm) and the 6x6x6
+//             node window of each page not staged yet                    (data)
 //   unit k  : computed from shared memory
-// so global latency is hidden behind the previous unit's arithmetic.
+// so global latency is hidden behind the previous unit's arithmetic.  Pages
+// are numbered in the order the CTA meets them; a page's window sits in ring
+// slot seq mod kWinRing and its adjacency row and key in slot seq mod
+// kPageRing (units k .. k+2 span at most 9 pages, units k and k+1 at most 6).
 constexpr int kG2PUnit = 256;
 constexpr int kG2PMinBlocks = 2;  // resident CTAs per SM (FP32), bounded by registers
 constexpr int kPlanesR = 16;  // x0..2, F0..8, c, alpha, psi, m
+constexpr int kUnitPages = 3;
+constexpr int kWinRing = 8;
+constexpr int kPageRing = 16;
+
+// Unit descriptor fields in shared memory.
+enum : int { UD_S0 = 0, UD_N = 1, UD_SEQ = 2, UD_NP = 3, UD_C1 = 4, UD_C2 = 5, UD_P0 = 6, UD_WORDS = 8 };
 
 template <typename R>
 struct G2PShared {
-    R win4[2][kWindowNodes][4];  // (v0, v1, v2, dc) per window node; 2 page buffers
-    R wincn[2][kWindowNodes];    // c_new per window node
-    R p[2][kPlanesR][kG2PUnit];  // staged particle inputs; 2 unit buffers
+    R win4[kWinRing][kWindowNodes][4];  // (v0, v1, v2, dc) per window node
+    R wincn[kWinRing][kWindowNodes];    // c_new per window node
+    R p[2][kPlanesR][kG2PUnit];          // staged particle inputs; 2 unit buffers
     uint32_t id[2][kG2PUnit];
-    int32_t o[3][kG2PUnit];      // previous slot per unit slot; 3 meta buffers
+    int32_t o[3][kG2PUnit];              // previous slot per unit slot; 3 meta buffers
     uint32_t key[3][kG2PUnit];
-    int32_t adj[3][8];
-    uint32_t bkey[3];
-    int32_t unit[3][4];          // page, first slot, count (0: none), window buffer
+    int32_t adj[kPageRing][8];
+    uint32_t bkey[kPageRing];
+    int32_t unit[3][UD_WORDS];
 };
 
 enum : int { P_X = 0, P_F = 3, P_C = 12, P_ALPHA = 13, P_PSI = 14, P_M = 15 };
@@ -62,63 +75,93 @@ __device__ __forceinline__ void bspline1d_g(R xp, R inv_dx, R* w, R* g) {
     g[2] = z * inv_dx;
 }
 
-// Unit sequence of one CTA: its pages blockIdx.x + k gridDim.x, each cut into
-// runs of kG2PUnit slots.  Every thread runs the same iterator.
+// Unit sequence of one CTA: slots [b T / C, (b + 1) T / C) of the T sorted
+// slots, C = gridDim.x, in units of up to kG2PUnit slots and kUnitPages pages.
+// Every thread runs the same iterator in step (it shuffles), so it is called
+// by all threads of the CTA at the same points.  Page starts cs(q) =
+// cell_start[64 q] are held 32 pages at a time in lane registers, the next
+// 32 prefetched.
 struct UnitIter {
-    int page, next, end;      // current page, next run start, page end
-    int nbs, nbe;             // slot range of the following page (loaded one page ahead)
-    __device__ void init(const BinDev& bin, int nb) {
-        page = blockIdx.x;
-        next = end = 0;
-        if (page < nb) {
-            next = bin.cell_start[(int64_t)page * 64];
-            end = bin.cell_start[(int64_t)page * 64 + 64];
-        }
-        preload(bin, nb);
+    int64_t s, se;    // next unit start, end of the CTA's share
+    int p, seq;       // page containing s and its sequence number
+    int nb, total;
+    int P0;           // first page of the lane-held block
+    int cur, nxt;     // cs(P0 + lane), cs(P0 + 32 + lane)
+    __device__ int load_cs(const BinDev& bin, int q) const {
+        q = min(q, nb);
+        return bin.cell_start[(int64_t)q * 64];
     }
-    __device__ void preload(const BinDev& bin, int nb) {
-        const int q = page + (int)gridDim.x;
-        nbs = nbe = 0;
-        if (q < nb) {
-            nbs = bin.cell_start[(int64_t)q * 64];
-            nbe = bin.cell_start[(int64_t)q * 64 + 64];
-        }
+    __device__ void init(const BinDev& bin, int nb_) {
+        nb = nb_;
+        total = nb > 0 ? bin.cell_start[(int64_t)nb * 64] : 0;
+        s = (int64_t)blockIdx.x * total / gridDim.x;
+        se = (int64_t)(blockIdx.x + 1) * total / gridDim.x;
+        p = 0;
+        if (s < se) p = bin.page_rank[bin.keys_sorted[s] >> 6];
+        seq = 0;
+        P0 = p;
+        const int lane = threadIdx.x & 31;
+        cur = load_cs(bin, P0 + lane);
+        nxt = load_cs(bin, P0 + 32 + lane);
     }
-    // Next unit (page, first slot, count); count 0 when the CTA is done.
-    __device__ void step(const BinDev& bin, int nb, int& b, int& s0, int& n) {
-        while (page < nb && next >= end) {
-            page += gridDim.x;
-            next = nbs;
-            end = nbe;
-            if (page < nb) preload(bin, nb);
+    // cs(q) for P0 <= q < P0 + 64
+    __device__ int cs(int q) const {
+        const int r = q - P0;
+        const int lo = __shfl_sync(0xffffffffu, cur, r & 31);
+        const int hi = __shfl_sync(0xffffffffu, nxt, r & 31);
+        return r < 32 ? lo : hi;
+    }
+    // Next unit; n = 0 when the CTA is done.
+    __device__ void step(const BinDev& bin, int& s0, int& n, int& seq0, int& np, int& c1, int& c2, int& p0) {
+        // keep p in the first block, so that p .. p + kUnitPages lie in the two
+        while (p >= P0 + 32) {
+            P0 += 32;
+            cur = nxt;
+            nxt = load_cs(bin, P0 + 32 + (int)(threadIdx.x & 31));
         }
-        if (page < nb) {
-            b = page;
-            s0 = next;
-            n = min(kG2PUnit, end - next);
-            next += kG2PUnit;
-        } else {
-            b = -1;
-            s0 = 0;
-            n = 0;
+        if (s >= se) {
+            s0 = n = seq0 = np = c1 = c2 = p0 = 0;
+            return;
         }
+        const int a1 = cs(p + 1), a2 = cs(p + 2), a3 = cs(p + 3);
+        int64_t e = min(s + kG2PUnit, se);
+        if (a3 < e) e = a3;
+        s0 = (int)s;
+        n = (int)(e - s);
+        seq0 = seq;
+        p0 = p;
+        np = 1 + (a1 < e) + (a2 < e);
+        c1 = a1;
+        c2 = a2;
+        const int adv = (a1 <= e) + (a2 <= e) + (a3 <= e);
+        p += adv;
+        seq += adv;
+        s = e;
     }
 };
 
 template <typename R>
-__device__ __forceinline__ void issue_meta(G2PShared<R>& S, int m, int b, int s0, int n, const BinDev& bin) {
+__device__ __forceinline__ void issue_meta(G2PShared<R>& S, int m, int s0, int n, int seq0, int np, int p0,
+                                           const BinDev& bin) {
     const int t = threadIdx.x;
     if (n <= 0) return;
     if (t < n) {
         cp_async_elem(&S.o[m][t], &bin.perm[s0 + t]);
         cp_async_elem(&S.key[m][t], &bin.keys_sorted[s0 + t]);
     }
-    if (t < 8) cp_async_elem(&S.adj[m][t], &bin.adj[(int64_t)b * 8 + t]);
-    if (t == 8) cp_async_elem(&S.bkey[m], &bin.block_keys[b]);
+    if (t < 8 * np) {
+        const int j = t >> 3;
+        cp_async_elem(&S.adj[(seq0 + j) % kPageRing][t & 7], &bin.adj[(int64_t)(p0 + j) * 8 + (t & 7)]);
+    } else if (t < 8 * kUnitPages + np && t >= 8 * kUnitPages) {
+        const int j = t - 8 * kUnitPages;
+        cp_async_elem(&S.bkey[(seq0 + j) % kPageRing], &bin.block_keys[p0 + j]);
+    }
 }
 
+// Particle inputs of a unit, and the windows of its pages with sequence
+// numbers in [wseq0, wseq1) (the pages not staged by the previous unit).
 template <typename R>
-__device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int n, bool window, int wbuf,
+__device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int n, int wseq0, int wseq1,
                                            const PState<R>& in, const R* __restrict__ nodes) {
     const int t = threadIdx.x;
     if (t < n) {
@@ -133,13 +176,15 @@ __device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int 
         cp_async_elem(&S.p[buf][P_M][t], in.m + o);
         cp_async_elem(&S.id[buf][t], in.id + o);
     }
-    if (window) {
+    for (int wseq = wseq0; wseq < wseq1; ++wseq) {
+        const int wbuf = wseq % kWinRing;
+        const int32_t* adj = S.adj[wseq % kPageRing];
         for (int w = t; w < kGridChannels * kWindowNodes; w += kG2PUnit) {
             const int ch = w / kWindowNodes;
             const int node = w - ch * kWindowNodes;
             const int a = node / 36, bb = (node / 6) % 6, cc = node % 6;
             const int d = ((a >> 2) << 2) | ((bb >> 2) << 1) | (cc >> 2);
-            const int g = S.adj[m][d];
+            const int g = adj[d];
             R* dst = (ch < 4) ? &S.win4[wbuf][node][ch] : &S.wincn[wbuf][node];
             if (g >= 0)
                 cp_async_elem(dst, nodes + (int64_t)g * kGridChannels * 64 + ch * 64 + (a & 3) * 16 + (bb & 3) * 4 +
@@ -167,47 +212,58 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
     // prologue: meta of units 0 and 1, data of unit 0
     UnitIter it;
     it.init(bin, nb);
-    int b0, s00, n0, b1, s01, n1;
-    it.step(bin, nb, b0, s00, n0);
-    it.step(bin, nb, b1, s01, n1);
+    int d0[7], d1[7];  // s0, n, seq0, np, c1, c2, p0
+    it.step(bin, d0[0], d0[1], d0[2], d0[3], d0[4], d0[5], d0[6]);
+    it.step(bin, d1[0], d1[1], d1[2], d1[3], d1[4], d1[5], d1[6]);
     if (t == 0) {
-        S.unit[0][0] = b0; S.unit[0][1] = s00; S.unit[0][2] = n0; S.unit[0][3] = 0;
-        S.unit[1][0] = b1; S.unit[1][1] = s01; S.unit[1][2] = n1; S.unit[1][3] = (b1 == b0) ? 0 : 1;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            S.unit[0][q] = d0[q];
+            S.unit[1][q] = d1[q];
+        }
     }
-    issue_meta(S, 0, b0, s00, n0, bin);
+    issue_meta(S, 0, d0[0], d0[1], d0[2], d0[3], d0[6], bin);
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
-    issue_data(S, 0, 0, n0, n0 > 0, 0, in, nodes);
-    issue_meta(S, 1, b1, s01, n1, bin);
+    int staged = d0[2] + d0[3];  // pages with sequence numbers below this have their window staged
+    issue_data(S, 0, 0, d0[1], d0[1] > 0 ? d0[2] : 0, d0[1] > 0 ? staged : 0, in, nodes);
+    issue_meta(S, 1, d1[0], d1[1], d1[2], d1[3], d1[6], bin);
     cp_async_commit();
 
     for (int k = 0;; ++k) {
         cp_async_wait_all();
         __syncthreads();
         const int m0 = k % 3, m1 = (k + 1) % 3, m2 = (k + 2) % 3;
-        const int u0b = S.unit[m0][0], u0s = S.unit[m0][1], u0n = S.unit[m0][2], u0w = S.unit[m0][3];
+        const int u0s = S.unit[m0][UD_S0], u0n = S.unit[m0][UD_N], u0seq = S.unit[m0][UD_SEQ];
+        const int u0c1 = S.unit[m0][UD_C1], u0c2 = S.unit[m0][UD_C2], u0np = S.unit[m0][UD_NP];
         if (u0n <= 0) break;
         {
             // unit k+2: iterator step, descriptor and meta; unit k+1: data
-            int b2, s02, n2;
-            it.step(bin, nb, b2, s02, n2);
-            const int u1b = S.unit[m1][0], u1n = S.unit[m1][2], u1w = S.unit[m1][3];
+            int d2[7];
+            it.step(bin, d2[0], d2[1], d2[2], d2[3], d2[4], d2[5], d2[6]);
+            const int u1n = S.unit[m1][UD_N], u1seq = S.unit[m1][UD_SEQ], u1np = S.unit[m1][UD_NP];
             if (t == 0) {
-                S.unit[m2][0] = b2;
-                S.unit[m2][1] = s02;
-                S.unit[m2][2] = n2;
-                S.unit[m2][3] = (b2 == u1b) ? u1w : 1 - u1w;
+#pragma unroll
+                for (int q = 0; q < 7; ++q) S.unit[m2][q] = d2[q];
             }
-            issue_data(S, m1, (k + 1) & 1, u1n, u1n > 0 && u1b != u0b, u1w, in, nodes);
-            issue_meta(S, m2, b2, s02, n2, bin);
+            int w0 = 0, w1 = 0;
+            if (u1n > 0) {
+                w0 = max(u1seq, staged);
+                w1 = u1seq + u1np;
+                staged = max(staged, w1);
+            }
+            issue_data(S, m1, (k + 1) & 1, u1n, w0, w1, in, nodes);
+            issue_meta(S, m2, d2[0], d2[1], d2[2], d2[3], d2[6], bin);
             cp_async_commit();
         }
         if (t < u0n) {
             const int buf = k & 1;
             const int slot = u0s + t;
+            // the particle's page within the unit
+            const int pseq = u0seq + (u0np > 1 && slot >= u0c1) + (u0np > 2 && slot >= u0c2);
             int bx, by, bz;
-            page_coords(S.bkey[m0], bx, by, bz);
+            page_coords(S.bkey[pseq % kPageRing], bx, by, bz);
             const uint32_t cell = S.key[m0][t] & 63u;
             const int li = (int)(cell >> 4), lj = (int)((cell >> 2) & 3), lk = (int)(cell & 3);
             const R x[3] = {S.p[buf][P_X][t], S.p[buf][P_X + 1][t], S.p[buf][P_X + 2][t]};
@@ -232,8 +288,8 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
                 wyd[q] = wy[q] * (R(q) * dx - xp[1]);
                 wzd[q] = wz[q] * (R(q) * dx - xp[2]);
             }
-            const R(*win4)[4] = S.win4[u0w];
-            const R* wincn = S.wincn[u0w];
+            const R(*win4)[4] = S.win4[pseq % kWinRing];
+            const R* wincn = S.wincn[pseq % kWinRing];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 // sums over j for this i: T0 (Y Z), Ty (Y' Z), Tz (Y Z'), Tdy (Y d Z), Tdz (Y Z d)
@@ -413,7 +469,8 @@ cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, cons
                        const PState<R>& in, const PState<R>& out, const PAux<R>& aux, BinDev bin, GridDev grid,
                        Counters* cnt, LaunchCfg cfg, cudaStream_t stream) {
     const int per_sm = sizeof(R) == 4 ? kG2PMinBlocks : 1;
-    const int ctas = max(1, min(bin.nb_cap, cfg.num_sms * per_sm));
+    const int64_t units = (bin.n + kG2PUnit - 1) / kG2PUnit;
+    const int ctas = (int)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)cfg.num_sms * per_sm));
     k_g2p<R><<<ctas, kG2PUnit, sizeof(G2PShared<R>), stream>>>(sc, fallback64, in, out, aux, bin,
                                                reinterpret_cast<const R*>(grid.nodes), cnt);
     k_advance_time<R><<<1, 1, 0, stream>>>(cnt, const_cast<SceneDev<R>*>(sc), const_cast<SceneDev<double>*>(sc64));
