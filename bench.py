@@ -188,6 +188,24 @@ class ClockSampler:
                     samples=len(sm))
 
 
+def max_over_ranks(value: float, dist, device=None) -> float:
+    """Largest per-rank value over all ranks: a job's time is its slowest rank's.
+    The reduction runs on `device` under NCCL and on the host under gloo."""
+    if dist is None:
+        return float(value)
+    import torch
+    on = device if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=on)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, particles: int, steps: int, ms_max: float) -> float:
+    """Whole-job particle-substeps/s of `world` replicas of `particles` particles
+    stepped `steps` substeps, timed as the slowest rank's `ms_max`."""
+    return world * particles * steps / (ms_max / 1e3)
+
+
 def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
     import torch
 
@@ -228,11 +246,8 @@ def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
     diag = scene.diagnostics()
     launches = diag["kernel_launches"] - launches0
     status = scene.sync()
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * sp.n * args.steps / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist, dev)
+    value = job_rate(world, sp.n, args.steps, ms_max)
 
     # per-stage device times (CUDA events on the same stream) for the roofline
     stages = scene.substep_timed(min(5, max(1, args.steps)), sh)
@@ -286,17 +301,14 @@ def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
             e1.record(stream)
             e1.synchronize()
             barrier()
-            t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-            if dist is not None:
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
+            return max_over_ranks(e0.elapsed_time(e1), dist, dev)
 
         e_ms = frame_loop(True)
         b_ms = frame_loop(False)
         bc_bytes = sizeof_velocity_conditions(np.float32)
-        e2e = dict(value=world * sp.n * args.steps / (e_ms / 1e3), unit="particle-substeps/s",
+        e2e = dict(value=job_rate(world, sp.n, args.steps, e_ms), unit="particle-substeps/s",
                    h2d_bytes_per_step=bc_bytes, d2h_bytes_per_step=sp.n * 16,
-                   blocking_value=world * sp.n * args.steps / (b_ms / 1e3),
+                   blocking_value=job_rate(world, sp.n, args.steps, b_ms),
                    note="per step: velocity conditions H2D (pinned), gmpm_substep, positions+damage FP32 D2H "
                         "(pinned) through the C-ABI, as MPMSimulator::simulateStick + Attribs_Back_Host; reads "
                         "overlapped with the next substep (gmpm_read_particles_async, all landed at the end); "

@@ -1,0 +1,77 @@
+"""The multi-GPU form of the path is independent replicas, one per rank, with
+no collective on the data path: ranks meet only at the timing barriers, and
+the job's time is the slowest rank's.  These tests run that host-side logic
+of bench.py as two gloo ranks on the CPU."""
+from __future__ import annotations
+
+import importlib.util
+import os
+import socket
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _load_bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int, out_dir: str):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        bench = _load_bench()
+        local_ms = 100.0 + 25.0 * rank  # rank 1 is the slow one
+        dist.barrier()
+        ms_max = bench.max_over_ranks(local_ms, dist)
+        rate = bench.job_rate(world, 1000, 10, ms_max)
+        dist.barrier()
+        Path(out_dir, f"rank{rank}.txt").write_text(f"{ms_max} {rate}")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_slowest_rank_sets_the_job_time(tmp_path):
+    import torch.multiprocessing as mp
+
+    world = 2
+    mp.spawn(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    for rank in range(world):
+        ms_max, rate = map(float, Path(tmp_path, f"rank{rank}.txt").read_text().split())
+        assert ms_max == 125.0
+        # two replicas of 1000 particles, 10 substeps each, in 125 ms
+        assert rate == pytest.approx(2 * 1000 * 10 / 0.125)
+
+
+def test_single_process_needs_no_group():
+    bench = _load_bench()
+    assert bench.max_over_ranks(42.5, None) == 42.5
+    assert bench.job_rate(1, 500, 4, 2.0) == pytest.approx(1e6)
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    """Under torchrun the reference (CPU) arm prints its line from rank 0 only;
+    other ranks exit 0 without work or output."""
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1"],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == ""
