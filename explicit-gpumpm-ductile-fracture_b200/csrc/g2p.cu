@@ -55,6 +55,9 @@ struct G2PShared {
     int32_t adj[kPageRing][8];
     uint32_t bkey[kPageRing];
     int32_t unit[3][UD_WORDS];
+    // per window value w = ch * 216 + node: source offset in its grid page
+    // (bits 0-8), neighbour slot (9-11), destination offset (12-21), c_new flag (22)
+    uint32_t wtab[kGridChannels * kWindowNodes];
 };
 
 enum : int { P_X = 0, P_F = 3, P_C = 12, P_ALPHA = 13, P_PSI = 14, P_M = 15 };
@@ -180,15 +183,12 @@ __device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int 
         const int wbuf = wseq % kWinRing;
         const int32_t* adj = S.adj[wseq % kPageRing];
         for (int w = t; w < kGridChannels * kWindowNodes; w += kG2PUnit) {
-            const int ch = w / kWindowNodes;
-            const int node = w - ch * kWindowNodes;
-            const int a = node / 36, bb = (node / 6) % 6, cc = node % 6;
-            const int d = ((a >> 2) << 2) | ((bb >> 2) << 1) | (cc >> 2);
-            const int g = adj[d];
-            R* dst = (ch < 4) ? &S.win4[wbuf][node][ch] : &S.wincn[wbuf][node];
+            const uint32_t e = S.wtab[w];
+            const int g = adj[(e >> 9) & 7];
+            const int off = (int)((e >> 12) & 1023);
+            R* dst = (e >> 22) ? &S.wincn[wbuf][off] : &S.win4[wbuf][0][0] + off;
             if (g >= 0)
-                cp_async_elem(dst, nodes + (int64_t)g * kGridChannels * 64 + ch * 64 + (a & 3) * 16 + (bb & 3) * 4 +
-                                       (cc & 3));
+                cp_async_elem(dst, nodes + (int64_t)g * kGridChannels * 64 + (e & 511));
             else
                 *dst = R(0);
         }
@@ -224,6 +224,16 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
     }
     issue_meta(S, 0, d0[0], d0[1], d0[2], d0[3], d0[6], bin);
     cp_async_commit();
+    // window copy table, once per CTA (the divisions of the node index)
+    for (int w = t; w < kGridChannels * kWindowNodes; w += kG2PUnit) {
+        const int ch = w / kWindowNodes;
+        const int node = w - ch * kWindowNodes;
+        const int a = node / 36, bb = (node / 6) % 6, cc = node % 6;
+        const int d = ((a >> 2) << 2) | ((bb >> 2) << 1) | (cc >> 2);
+        const uint32_t src = (uint32_t)(ch * 64 + (a & 3) * 16 + (bb & 3) * 4 + (cc & 3));
+        const uint32_t dst = (uint32_t)(ch < 4 ? node * 4 + ch : node);
+        S.wtab[w] = src | ((uint32_t)d << 9) | (dst << 12) | ((uint32_t)(ch == 4) << 22);
+    }
     cp_async_wait_all();
     __syncthreads();
     int staged = d0[2] + d0[3];  // pages with sequence numbers below this have their window staged
