@@ -12,8 +12,8 @@
 // Determinism: dot products are partial sums over runs of 128 entries in a
 // fixed tree order, combined in a fixed order (by max instead of a sum when
 // the reference's getDotProduct quirk is selected, :727-743), and K x is
-// gathered per node in fixed cell and particle order, so runs are bitwise
-// reproducible.
+// summed per cell z-column and gathered per node in a fixed order, so runs
+// are bitwise reproducible.
 #include <cstdint>
 
 #include "kernels.h"
@@ -23,8 +23,10 @@ namespace gmpm {
 constexpr int kPcgBlock = 128;     // vector entries per partial sum (2 grid pages)
 constexpr int kPcgScalarThreads = 1024;
 constexpr int kPcgColThreads = 256;
-constexpr int kPcgKxThreads = 256;
+constexpr int kPcgKxWarps = 16;    // one per cell z-column of a page
+constexpr int kPcgKxThreads = 32 * kPcgKxWarps;
 constexpr int kPcgKxChunk = 512;   // particles staged per pass of a page
+constexpr int kKxRec = 11;         // staged per particle: xp0, xp1, wz[3], gz[3], col[3]
 
 // ---- helpers -----------------------------------------------------------------
 
@@ -181,28 +183,80 @@ __global__ void __launch_bounds__(kPcgColThreads)
     }
 }
 
-// Page tile of K s: window node (a, b, c) gathers grad w . col over the
-// particles of the page's cells whose stencil covers it, in cell then slot
-// order (the sorted particle order of the scatter, AxP2G_APIC).
+// x or y B-spline piece of stencil node k for one lane, branch-free:
+// w = a z^2 + b and dw/dx = c z with z = xp/dx - shift.
+struct KxPiece {
+    double shift, a, b, c;
+    __device__ void init(int k, double inv_dx) {
+        shift = k == 0 ? 1.5 : (k == 1 ? 1.0 : 0.5);
+        a = k == 1 ? -1.0 : 0.5;
+        b = k == 1 ? 0.75 : 0.0;
+        c = (k == 1 ? -2.0 : 1.0) * inv_dx;
+    }
+    __device__ __forceinline__ void eval(double xp, double inv_dx, double& w, double& g) const {
+        const double z = xp * inv_dx - shift;
+        w = a * (z * z) + b;
+        g = c * z;
+    }
+};
+
+// One particle of cell z-index CZ into the lane's six z-node sums:
+// grad w . col = wz (gx wy c0 + wx gy c1) + gz (wx wy c2).
+template <int CZ>
+__device__ __forceinline__ void kx_accumulate(const double* __restrict__ r, const KxPiece& px, const KxPiece& py,
+                                              double inv_dx, double* acc) {
+    double wx, gx, wy, gy;
+    px.eval(r[0], inv_dx, wx, gx);
+    py.eval(r[1], inv_dx, wy, gy);
+    const double u = gx * wy * r[8] + wx * gy * r[9];
+    const double v = wx * wy * r[10];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[CZ + k] += r[2 + k] * u + r[5 + k] * v;
+}
+
+template <int CZ>
+__device__ __forceinline__ void kx_cell(const double* __restrict__ recs, const int* __restrict__ cs, int cb, int c0,
+                                        int c1, int sub, const KxPiece& px, const KxPiece& py, double inv_dx,
+                                        double* acc) {
+    const int lo = max(cs[cb + CZ], c0) - c0, hi = min(cs[cb + CZ + 1], c1) - c0;
+#pragma unroll 2
+    for (int p = lo + sub; p < hi; p += 3) kx_accumulate<CZ>(recs + (size_t)p * kKxRec, px, py, inv_dx, acc);
+}
+
+// Page tile of K s (AxP2G_APIC): window node (a, b, c) sums grad w . col over
+// the particles whose stencil covers it.  As in the P2G: one warp per cell
+// z-column (cx, cy); lane (sub, i, j) = particle stream sub (the warp takes
+// three particles of a cell per step) x stencil column (i, j), with the sums
+// of window nodes (cx+i, cy+j, 0..5) in registers.  At the page's end the
+// three streams of a stencil column are added in fixed order, and each window
+// node gathers its (at most 4) columns in fixed order, compensated, so runs
+// are bitwise reproducible.
 template <typename R>
 __global__ void __launch_bounds__(kPcgKxThreads)
     k_pcg_kx(const SceneDev<R>* __restrict__ sc, PState<R> st, BinDev bin, PcgDev P, double* __restrict__ tile,
              const Counters* __restrict__ cnt) {
     if (P.scal->done) return;
-    __shared__ double xs[kPcgKxChunk][3];
-    __shared__ double cs[kPcgKxChunk][3];
+    __shared__ double recs[kPcgKxChunk * kKxRec];  // staged particles; the column sums at a page's end
     __shared__ int cstart[65];
+    static_assert(16 * 9 * 6 <= kPcgKxChunk * kKxRec, "column sums fit the staging buffer");
     const int nb = min(cnt->n_blocks, bin.nb_cap);
     const double dx = sc->dx_d, inv_dx = sc->inv_dx_d;
-    const int t = threadIdx.x;
-    const int na = t / 36, nbb = (t / 6) % 6, nc = t % 6;  // window node of this thread (t < 216)
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int le = lane < 27 ? lane : lane - 27;  // lanes 27..31 shadow lanes 0..4 and never write
+    const int sub = le / 9, col = le - sub * 9;
+    const int ci = col / 3, cj = col - ci * 3;
+    const int wcx = warp >> 2, wcy = ((warp & 3) - wcx) & 3;  // one column of every cx and cy per scheduler
+    const int cb = wcx * 16 + wcy * 4;
+    KxPiece px, py;
+    px.init(ci, inv_dx);
+    py.init(cj, inv_dx);
     for (int b = blockIdx.x; b < nb; b += gridDim.x) {
         __syncthreads();
         for (int q = t; q < 65; q += kPcgKxThreads) cstart[q] = bin.cell_start[(int64_t)b * 64 + q];
         int bx, by, bz;
         page_coords(bin.block_keys[b], bx, by, bz);
         __syncthreads();
-        double acc = 0.0;
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int c0 = cstart[0]; c0 < cstart[64]; c0 += kPcgKxChunk) {
             const int c1 = min(cstart[64], c0 + kPcgKxChunk);
             __syncthreads();
@@ -211,32 +265,43 @@ __global__ void __launch_bounds__(kPcgKxThreads)
                 const uint32_t cell = bin.keys_sorted[slot] & 63u;
                 const int base[3] = {4 * bx + (int)(cell >> 4), 4 * by + (int)((cell >> 2) & 3),
                                      4 * bz + (int)(cell & 3)};
+                double* r = recs + (size_t)(slot - c0) * kKxRec;
+                r[0] = (double)st.x[0][o] - (double)base[0] * dx;
+                r[1] = (double)st.x[1][o] - (double)base[1] * dx;
+                const double xp2 = (double)st.x[2][o] - (double)base[2] * dx;
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    xs[slot - c0][a] = (double)st.x[a][o] - (double)base[a] * dx;
-                    cs[slot - c0][a] = P.col[(int64_t)a * P.n + slot];
-                }
+                for (int k = 0; k < 3; ++k) bspline_k(xp2, inv_dx, k, r[2 + k], r[5 + k]);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) r[8 + a] = P.col[(int64_t)a * P.n + slot];
             }
             __syncthreads();
-            if (t < kWindowNodes) {
-                for (int cx = max(0, na - 2); cx <= min(3, na); ++cx)
-                    for (int cy = max(0, nbb - 2); cy <= min(3, nbb); ++cy)
-                        for (int cz = max(0, nc - 2); cz <= min(3, nc); ++cz) {
-                            const int cell = cx * 16 + cy * 4 + cz;
-                            const int lo = max(cstart[cell], c0), hi = min(cstart[cell + 1], c1);
-                            for (int p = lo; p < hi; ++p) {
-                                const double* xp = xs[p - c0];
-                                const double* cp = cs[p - c0];
-                                double wx, gx, wy, gy, wz, gz;
-                                bspline_k(xp[0], inv_dx, na - cx, wx, gx);
-                                bspline_k(xp[1], inv_dx, nbb - cy, wy, gy);
-                                bspline_k(xp[2], inv_dx, nc - cz, wz, gz);
-                                acc += gx * wy * wz * cp[0] + wx * gy * wz * cp[1] + wx * wy * gz * cp[2];
-                            }
-                        }
-            }
+            kx_cell<0>(recs, cstart, cb, c0, c1, sub, px, py, inv_dx, acc);
+            kx_cell<1>(recs, cstart, cb, c0, c1, sub, px, py, inv_dx, acc);
+            kx_cell<2>(recs, cstart, cb, c0, c1, sub, px, py, inv_dx, acc);
+            kx_cell<3>(recs, cstart, cb, c0, c1, sub, px, py, inv_dx, acc);
         }
-        if (t < kWindowNodes) tile[(int64_t)b * kWindowNodes + t] = acc;
+        // the three particle streams of a stencil column, in fixed order
+#pragma unroll
+        for (int z = 0; z < 6; ++z) {
+            const double v1 = __shfl_sync(0xffffffffu, acc[z], (lane + 9) & 31);
+            const double v2 = __shfl_sync(0xffffffffu, acc[z], (lane + 18) & 31);
+            acc[z] = (acc[z] + v1) + v2;
+        }
+        __syncthreads();  // every warp is past its sweep: the staging buffer is free
+        double* colsum = recs;  // [column 4 cx + cy][stencil column][z]
+        if (lane < 9) {
+#pragma unroll
+            for (int z = 0; z < 6; ++z) colsum[((wcx * 4 + wcy) * 9 + col) * 6 + z] = acc[z];
+        }
+        __syncthreads();
+        if (t < kWindowNodes) {
+            const int na = t / 36, nbb = (t / 6) % 6, nc = t % 6;
+            double sum = 0.0, comp = 0.0;
+            for (int cx = max(0, na - 2); cx <= min(3, na); ++cx)
+                for (int cy = max(0, nbb - 2); cy <= min(3, nbb); ++cy)
+                    kahan_add(sum, comp, colsum[((cx * 4 + cy) * 9 + (na - cx) * 3 + (nbb - cy)) * 6 + nc]);
+            tile[(int64_t)b * kWindowNodes + t] = sum;
+        }
     }
 }
 
