@@ -205,16 +205,18 @@ __device__ __forceinline__ void accumulate(const R* __restrict__ rec, int g, con
     const R al = bw[4] * gxy0 + bw[5] * gxy1, be = bw[6] * wxy;
     const R s1w = bw[7] * wxy;
     const R gam = bw[8] * wxy + bw[9] * gxy0 + bw[10] * gxy1, del = bw[11] * wxy;
-    R u = bw[0] + bw[1] * fi + bw[2] * fj;
+    // momentum at node k: wz (wxy u_k + al) + gz be with u_k = u0 + k A2, i.e.
+    // wz (alpha + k beta) + gz be
+    const R u0 = bw[0] + bw[1] * fi + bw[2] * fj;
+    const R alpha = wxy * u0 + al, beta = wxy * bw[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const R wz = cw[RF_WZ + k], gz = cw[RF_GZ + k];
-        const R w = wxy * wz;
+        const R tk = k == 0 ? alpha : (k == 1 ? alpha + beta : alpha + R(2) * beta);
         R* A = acc + 3 * (CZ + k);
-        A[0] += w * u + al * wz + be * gz;
+        A[0] += wz * tk + be * gz;
         A[1] += s1w * wz;
         A[2] += gam * wz + del * gz;
-        u += bw[3];
     }
 }
 
