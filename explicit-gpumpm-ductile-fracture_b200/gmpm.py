@@ -172,6 +172,10 @@ SIGNATURES = {
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
     "gmpm_generate_particles": (C.c_int, [C.POINTER(Geometry), C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                           C.POINTER(C.c_int32), C.c_int64]),
+    "gmpm_sample_obj": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int64]),
+    "gmpm_sample_cube": (C.c_int, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int64]),
+    "gmpm_sample_sdf": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_double, C.c_uint32,
+                                  C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int64]),
     "gmpm_scene_save": (C.c_int, [C.c_void_p, C.c_char_p]),
     "gmpm_scene_load": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
     "gmpm_batch_options_defaults": (None, [C.POINTER(BatchOptions)]),
@@ -249,6 +253,36 @@ def generate_particles(geom: Geometry) -> tuple[np.ndarray, np.ndarray]:
     check(L.gmpm_generate_particles(C.byref(geom), C.byref(n), _dptr(pos), _iptr(mat), n.value),
           "generate_particles")
     return pos, mat
+
+
+def _sampled(call, what: str) -> np.ndarray:
+    n = C.c_int64(0)
+    check(call(C.byref(n), None, 0), f"{what}(count)")
+    pos = np.empty((n.value, 3), dtype=np.float64)
+    check(call(C.byref(n), _dptr(pos), n.value), what)
+    return pos
+
+
+def sample_obj(path) -> np.ndarray:
+    """The reference's Sample::readObj: one particle per OBJ vertex record, y shifted by -0.2f."""
+    p = str(path).encode()
+    return _sampled(lambda n, out, cap: lib().gmpm_sample_obj(p, n, out, cap), "sample_obj")
+
+
+def sample_cube(n_grid: int) -> np.ndarray:
+    """The reference's Sample::Initialize_Data_cube on an n_grid^3 grid (27 particles per cell)."""
+    return _sampled(lambda n, out, cap: lib().gmpm_sample_cube(int(n_grid), n, out, cap), "sample_cube")
+
+
+def sample_sdf(path, center, res, dx: float, seed: int = 1) -> np.ndarray:
+    """The reference's Sample::Initial_data: rejection samples of an SDF level set placed in the
+    res[] grid cells around center[].  Draws from the C library's rand() after srand(seed), as the
+    reference does (seed 1 reproduces the reference's run)."""
+    p = str(path).encode()
+    c = (C.c_uint32 * 3)(*[int(v) for v in center])
+    r = (C.c_uint32 * 3)(*[int(v) for v in res])
+    return _sampled(lambda n, out, cap: lib().gmpm_sample_sdf(p, c, r, float(dx), int(seed), n, out, cap),
+                    "sample_sdf")
 
 
 class Context:

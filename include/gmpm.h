@@ -387,6 +387,30 @@ typedef struct gmpm_scene_geometry {
 gmpm_status gmpm_generate_particles(const gmpm_scene_geometry* geom, int64_t* count,
                                     double* positions, int32_t* material_ids, int64_t capacity);
 
+/* ---- the reference's scene samplers (host only) ----------------------------------------------
+ * Restatements of the reference's Sample class (GPU_MPM/LoadSample.cpp) that produce the same
+ * particles bit for bit.  Each is called first with positions == NULL for the count, then with
+ * capacity >= count; positions are xyz-interleaved doubles.  GMPM_IO_ERROR: the file cannot be read. */
+
+/* Sample::readObj (LoadSample.cpp:163-176): one particle per vertex, read as whitespace-separated
+ * "<char> x y z" records until a record fails to parse (so an "f a b c" record also yields a
+ * particle and a "vn"/"vt" record ends the list, as in the reference), with y shifted by -0.2f. */
+gmpm_status gmpm_sample_obj(const char* path, int64_t* count, double* positions, int64_t capacity);
+
+/* Sample::Initialize_Data_cube (LoadSample.cpp:179-213): the cells [N/2 - N/20, N/2 + N/20)^2 x
+ * [N/2 - N/8, N/2 + N/8) of an N^3 grid (dx = 1/N), 27 particles per cell on a 3x3x3 lattice of
+ * spacing dx/3 around the cell centre. */
+gmpm_status gmpm_sample_cube(int32_t n_grid, int64_t* count, double* positions, int64_t capacity);
+
+/* Sample::Initial_data (LoadSample.cpp:109-161): rejection samples of the level set in the SDF file
+ * (LoadSDF, :3-32: "ni nj nk", "minx miny minz", "dx", then ni*nj*nk values, i fastest), about 20
+ * per grid cell after scaling the level set into the res[] cells around center[] (grid spacing dx).
+ * The samples come from the C library's rand() after srand(seed), as the reference draws them from
+ * rand() (seed 1 is the generator's initial state, the reference's run): the call reseeds and
+ * advances the process-wide generator and is not thread-safe. */
+gmpm_status gmpm_sample_sdf(const char* path, const uint32_t center[3], const uint32_t res[3], double dx,
+                            uint32_t seed, int64_t* count, double* positions, int64_t capacity);
+
 /* ---- Checkpoint / resume ------------------------------------------------------------------------
  * A binary snapshot of a scene: its description, clock (time, substeps, current dt) and every particle
  * plane of the state in the internal order (the reference's Attribs_Back_Host, Particles.cpp:33-52,

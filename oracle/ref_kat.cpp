@@ -15,8 +15,17 @@
 //                         __GEIGEN__::math::msvd (QRSVD.hpp:327-374)
 //   material              read "E nu rho vol" lines, print lambda mu kappa M
 //                         (Materials.cpp:4-13)
+//   obj PATH              Sample::readObj (LoadSample.cpp:163-176) of PATH
+//   cube                  Sample::Initialize_Data_cube (LoadSample.cpp:179-213)
+//   sdf PATH cx cy cz rx ry rz
+//                         Sample::Initial_data (LoadSample.cpp:109-161) of the
+//                         SDF at PATH, with the C library generator in its
+//                         initial state, as in the reference's run
+// The sampling modes print the particle count, then one "%a %a %a" line per
+// particle.
 #include <math.h>  // brings the double overloads of abs() into the global namespace
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <iostream>
 #include <string>
@@ -26,12 +35,13 @@
 #include "QRSVD.hpp"
 #include "SPGridMask.h"
 #include "Materials.h"
+#include "LoadSample.h"
 
 static void print_hex(double v) { std::printf("%a", v); }
 
 int main(int argc, char** argv) {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: ref_kat masks|offsets|svd|material\n");
+        std::fprintf(stderr, "usage: ref_kat masks|offsets|svd|material|obj|cube|sdf\n");
         return 2;
     }
     std::string mode = argv[1];
@@ -87,6 +97,33 @@ int main(int argc, char** argv) {
             print_hex(m._mu); std::printf(" ");
             print_hex(m._kappa); std::printf(" ");
             print_hex(m.parabolic_M); std::printf("\n");
+        }
+        return 0;
+    }
+    if (mode == "obj" || mode == "cube" || mode == "sdf") {
+        Sample sample;
+        std::vector<vector3T> pts;
+        if (mode == "obj" && argc >= 3) {
+            pts = sample.readObj(argv[2]);
+        } else if (mode == "cube") {
+            pts = sample.Initialize_Data_cube();
+        } else if (mode == "sdf" && argc >= 9) {
+            unsigned int center[3], res[3];
+            for (int a = 0; a < 3; ++a) {
+                center[a] = (unsigned)std::atoi(argv[3 + a]);
+                res[a] = (unsigned)std::atoi(argv[6 + a]);
+            }
+            pts = sample.Initial_data(center, res, argv[2]);
+        } else {
+            std::fprintf(stderr, "bad arguments for %s\n", argv[1]);
+            return 2;
+        }
+        std::fflush(stdout);
+        std::printf("COUNT %zu\n", pts.size());
+        for (const vector3T& q : pts) {
+            print_hex(q.x); std::printf(" ");
+            print_hex(q.y); std::printf(" ");
+            print_hex(q.z); std::printf("\n");
         }
         return 0;
     }

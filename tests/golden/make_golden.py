@@ -10,6 +10,7 @@ the tests read the fixture.
 """
 from __future__ import annotations
 
+import hashlib
 import json
 import subprocess
 from pathlib import Path
@@ -56,6 +57,53 @@ def svd_inputs(rng: np.random.Generator) -> list[np.ndarray]:
     return mats
 
 
+GOLDEN = Path(__file__).resolve().parent
+TUBE = Path("/root/reference/Assets/sample/tube_10.obj")
+SDF_CENTER, SDF_RES = (128, 64, 128), (8, 8, 8)
+
+
+def write_sampler_inputs() -> None:
+    """Small committed inputs for the reference's samplers: a sphere level set
+    in the reference's SDF text format, and an OBJ with face and normal
+    records around its vertices."""
+    n = 16
+    g = np.arange(n, dtype=np.float64)
+    i, j, k = np.meshgrid(g, g, g, indexing="ij")
+    phi = np.sqrt((i - 7.3) ** 2 + (j - 7.8) ** 2 + (k - 8.1) ** 2) - 5.2
+    vals = phi.transpose(2, 1, 0).ravel()  # i fastest
+    lines = [f"{n} {n} {n}", "-0.5 -0.5 -0.5", "0.0625"] + [repr(float(v)) for v in vals]
+    (GOLDEN / "sample_sphere.sdf").write_text("\n".join(lines) + "\n")
+    rng = np.random.default_rng(5)
+    v = rng.uniform(0.0, 1.0, (120, 3)).tolist()
+    recs = [f"v {a!r} {b!r} {c!r}" for a, b, c in v[:100]]
+    recs += ["f 1 2 3", "f 4 5 6"] + [f"v {a!r} {b!r} {c!r}" for a, b, c in v[100:110]]
+    recs += ["vn 0 1 0"] + [f"v {a!r} {b!r} {c!r}" for a, b, c in v[110:]]
+    (GOLDEN / "sample_records.obj").write_text("\n".join(recs) + "\n")
+
+
+def sampler_record(args: list[str]) -> dict:
+    r = subprocess.run([str(REF), *args], capture_output=True, text=True, check=True)
+    lines = r.stdout.splitlines()
+    at = next(i for i, l in enumerate(lines) if l.startswith("COUNT"))
+    n = int(lines[at].split()[1])
+    pts = np.array([[float.fromhex(x) for x in l.split()] for l in lines[at + 1:at + 1 + n]], dtype=np.float64)
+    pts = pts.reshape(-1, 3)
+    return {"count": n, "sha1": hashlib.sha1(pts.tobytes()).hexdigest(),
+            "first": [x.hex() for x in pts[0]] if n else [], "last": [x.hex() for x in pts[-1]] if n else []}
+
+
+def sampler_kats() -> dict:
+    write_sampler_inputs()
+    out = {"sample_records_obj": sampler_record(["obj", str(GOLDEN / "sample_records.obj")]),
+           "sample_cube": sampler_record(["cube"]),
+           "sample_sdf": dict(center=SDF_CENTER, res=SDF_RES,
+                              **sampler_record(["sdf", str(GOLDEN / "sample_sphere.sdf"),
+                                                *map(str, SDF_CENTER), *map(str, SDF_RES)]))}
+    if TUBE.exists():
+        out["sample_tube_10_obj"] = sampler_record(["obj", str(TUBE)])
+    return out
+
+
 def main() -> None:
     if not REF.exists():
         subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True)
@@ -75,6 +123,7 @@ def main() -> None:
     svd_in = svd_inputs(rng)
     lines = run("svd", "\n".join(" ".join(float(x).hex() for x in A.ravel()) for A in svd_in) + "\n")
     out["svd"] = [{"F": [float(x).hex() for x in A.ravel()], "USV": l.split()[1:]} for A, l in zip(svd_in, lines)]
+    out.update(sampler_kats())
     OUT.write_text(json.dumps(out, separators=(",", ":")))
     print(f"wrote {OUT} ({len(out['svd'])} SVD cases, {len(out['offsets'])} offsets)")
 
