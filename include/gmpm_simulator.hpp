@@ -38,6 +38,44 @@ inline void gmpm_check(gmpm_status s, const char* what) {
     if (s != GMPM_OK) throw GmpmError(s, what);
 }
 
+// Scene sampling (GPU_MPM/LoadSample.h:10-24) over gmpm_sample_*: the same
+// particles as the reference's Sample, bit for bit.  The reference's grid
+// resolution N comes from Setting.h (256); here it is the constructor's.
+class Sample {
+  public:
+    explicit Sample(unsigned n_grid = 256) : N(n_grid) {}
+    std::vector<vector3T> readObj(std::string fileName) const {
+        return take([&](int64_t* n, double* p, int64_t cap) { return gmpm_sample_obj(fileName.c_str(), n, p, cap); },
+                    "gmpm_sample_obj");
+    }
+    std::vector<vector3T> Initialize_Data_cube() const {
+        return take([&](int64_t* n, double* p, int64_t cap) { return gmpm_sample_cube((int32_t)N, n, p, cap); },
+                    "gmpm_sample_cube");
+    }
+    // Draws from the C library's rand() after srand(seed) (seed 1: the reference's run).
+    std::vector<vector3T> Initial_data(unsigned int* center, unsigned int* res, std::string fileName,
+                                       unsigned seed = 1) const {
+        const uint32_t c[3] = {center[0], center[1], center[2]}, r[3] = {res[0], res[1], res[2]};
+        return take(
+            [&](int64_t* n, double* p, int64_t cap) {
+                return gmpm_sample_sdf(fileName.c_str(), c, r, 1.0 / N, seed, n, p, cap);
+            },
+            "gmpm_sample_sdf");
+    }
+    unsigned N;
+
+  private:
+    template <class F>
+    static std::vector<vector3T> take(F call, const char* what) {
+        int64_t n = 0;
+        gmpm_check(call(&n, nullptr, 0), what);
+        std::vector<vector3T> out((size_t)n);
+        static_assert(sizeof(vector3T) == 3 * sizeof(double), "vector3T is three doubles");
+        gmpm_check(call(&n, reinterpret_cast<double*>(out.data()), n), what);
+        return out;
+    }
+};
+
 // Material (GPU_MPM/Materials.h:15-23): constants live in the scene.
 class ElasticMaterial {
   public:

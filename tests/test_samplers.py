@@ -61,3 +61,25 @@ def test_sampler_errors(pkg):
     assert e.value.status == G.IO_ERROR
     with pytest.raises(G.GmpmError):
         G.sample_cube(2)
+
+
+def test_facade_sample_class_matches_reference(pkg, tmp_path):
+    """The C++ facade's Sample (the reference's class and method names) gives
+    the same particles as the reference's own LoadSample.cpp."""
+    import subprocess
+
+    root = Path(__file__).resolve().parents[1]
+    lib = pkg.gmpm.LIB_PATH
+    exe = tmp_path / "samples"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-I", str(root / "include"), str(root / "tests" / "cpp" /
+                    "samples.cpp"), str(lib), f"-Wl,-rpath,{lib.parent}", "-o", str(exe)], check=True)
+
+    def run(*args) -> np.ndarray:
+        out = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, check=True).stdout
+        lines = out.splitlines()
+        n = int(lines[0].split()[1])
+        return np.array([[float.fromhex(x) for x in l.split()] for l in lines[1:1 + n]], dtype=np.float64).reshape(-1, 3)
+
+    _check(run("obj", GOLDEN / "sample_records.obj"), GOLD["sample_records_obj"])
+    rec = GOLD["sample_sdf"]
+    _check(run("sdf", GOLDEN / "sample_sphere.sdf", *rec["center"], *rec["res"]), rec)
