@@ -227,6 +227,14 @@ struct Batch {
         return GMPM_OK;
     }
 
+    void set_launch_shapes(const int share[3], int nstreams) {
+        Candidate c{{share[0], share[1], share[2]}, nstreams > 0 ? nstreams : current.streams};
+        cands.clear();
+        tuned = true;
+        best = c;
+        apply(c);
+    }
+
     gmpm_status substep(int n, cudaStream_t s) {
         if (n < 0) return GMPM_INVALID_ARG;
         BATCH_TRY(cudaSetDevice(ctx->device));
@@ -345,6 +353,10 @@ void batch_destroy_deferred(gmpm_batch* b) {
     if (!b) return;
     cudaSetDevice(b->impl.ctx->device);
     delete b;
+}
+
+void batch_set_launch_shapes(gmpm_batch* b, const int share[3], int streams) {
+    if (b) b->impl.set_launch_shapes(share, streams);
 }
 }  // namespace gmpm
 

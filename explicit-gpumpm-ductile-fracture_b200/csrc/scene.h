@@ -66,6 +66,9 @@ struct SceneBase {
 
 // Destroy a batch without synchronising the device (its graphs may still run).
 void batch_destroy_deferred(gmpm_batch* b);
+// Fix a batch's launch shapes without tuning: SMs per scene by size class
+// (< 50k, < 200k, larger particles; 0: all) and the number of branches.
+void batch_set_launch_shapes(gmpm_batch* b, const int share[3], int streams);
 
 // Status of a set of device flags (GMPM_FLAG_*).
 gmpm_status flags_status(unsigned int flags);

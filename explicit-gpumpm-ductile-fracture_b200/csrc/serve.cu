@@ -137,6 +137,7 @@ struct Server {
     bool batch_stale = true;
     bool tuned = false;
     gmpm_batch_options tuned_opt{};
+    int tuned_share[3] = {0, 0, 0};  // SMs per scene by size class, from the first tuned batch
     int64_t next_id = 1;
     size_t used = 0;
     gmpm_server_stats st{};
@@ -333,6 +334,7 @@ struct Server {
         }
         gmpm_status s = gmpm_batch_create(ctx, hs.data(), (int)hs.size(), &o, &batch);
         if (s != GMPM_OK) return s;
+        if (tuned) batch_set_launch_shapes(batch, tuned_share, tuned_opt.streams);
         batch_stale = false;
         std::lock_guard<std::mutex> lk(mu);
         ++st.batches;
@@ -348,10 +350,11 @@ struct Server {
         tuned_opt = gmpm_batch_options{};
         tuned_opt.autotune = 0;
         tuned_opt.streams = info.streams;
-        // one share for all sizes when the tuner chose a single one; else the largest class's
-        tuned_opt.sm_share = info.sm_share_large ? info.sm_share_large
-                             : info.sm_share_medium ? info.sm_share_medium
-                                                    : info.sm_share_small;
+        // the tuned share of each size class (a class absent from the first
+        // batch keeps the whole device)
+        tuned_share[0] = info.sm_share_small;
+        tuned_share[1] = info.sm_share_medium;
+        tuned_share[2] = info.sm_share_large;
     }
 
     gmpm_status step(int n, cudaStream_t s) {
