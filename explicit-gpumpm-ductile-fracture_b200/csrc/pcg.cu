@@ -229,7 +229,7 @@ __device__ __forceinline__ void kx_cell(const double* __restrict__ recs, const i
 // three particles of a cell per step) x stencil column (i, j), with the sums
 // of window nodes (cx+i, cy+j, 0..5) in registers.  At the page's end the
 // three streams of a stencil column are added in fixed order, and each window
-// node gathers its (at most 4) columns in fixed order, compensated, so runs
+// node gathers its (at most 9) columns in fixed order, compensated, so runs
 // are bitwise reproducible.
 template <typename R>
 __global__ void __launch_bounds__(kPcgKxThreads)
