@@ -310,7 +310,8 @@ def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
                    h2d_bytes_per_step=bc_bytes, d2h_bytes_per_step=sp.n * 16,
                    blocking_value=job_rate(world, sp.n, args.steps, b_ms),
                    note="per step: velocity conditions H2D (pinned), gmpm_substep, positions+damage FP32 D2H "
-                        "(pinned) through the C-ABI, as MPMSimulator::simulateStick + Attribs_Back_Host; reads "
+                        "(pinned) through the C-ABI, as MPMSimulator::simulateStick + Attribs_Back_Host (which "
+                        "copies the same two fields as FP64 plus a colour word, 36 B/particle); reads "
                         "overlapped with the next substep (gmpm_read_particles_async, all landed at the end); "
                         "blocking_value: the same loop with gmpm_read_particles")
     return dict(sp=sp, what=what, value=value, ms_max=ms_max, launches=launches, clocks=clocks.summary(),
