@@ -23,7 +23,8 @@ namespace gmpm {
 constexpr int kPcgBlock = 128;     // vector entries per partial sum (2 grid pages)
 constexpr int kPcgScalarThreads = 1024;
 constexpr int kPcgColThreads = 256;
-constexpr int kPcgKxWarps = 16;    // one per cell z-column of a page
+constexpr int kPcgKxWarps = 8;     // two cell z-columns of a page each
+constexpr int kPcgKxCols = 16 / kPcgKxWarps;
 constexpr int kPcgKxThreads = 32 * kPcgKxWarps;
 constexpr int kPcgKxChunk = 512;   // particles staged per pass of a page
 constexpr int kKxRec = 11;         // staged per particle: xp0, xp1, wz[3], gz[3], col[3]
@@ -224,15 +225,16 @@ __device__ __forceinline__ void kx_cell(const double* __restrict__ recs, const i
 }
 
 // Page tile of K s (AxP2G_APIC): window node (a, b, c) sums grad w . col over
-// the particles whose stencil covers it.  As in the P2G: one warp per cell
-// z-column (cx, cy); lane (sub, i, j) = particle stream sub (the warp takes
+// the particles whose stencil covers it.  As in the P2G, per cell z-column
+// (cx, cy): eight warps own two columns each (small CTAs, four per SM, keep
+// more pages in flight); lane (sub, i, j) = particle stream sub (the warp takes
 // three particles of a cell per step) x stencil column (i, j), with the sums
 // of window nodes (cx+i, cy+j, 0..5) in registers.  At the page's end the
 // three streams of a stencil column are added in fixed order, and each window
 // node gathers its (at most 9) columns in fixed order, compensated, so runs
 // are bitwise reproducible.
 template <typename R>
-__global__ void __launch_bounds__(kPcgKxThreads)
+__global__ void __launch_bounds__(kPcgKxThreads, 4)
     k_pcg_kx(const SceneDev<R>* __restrict__ sc, PState<R> st, BinDev bin, PcgDev P, double* __restrict__ tile,
              const Counters* __restrict__ cnt) {
     if (P.scal->done) return;
@@ -245,8 +247,16 @@ __global__ void __launch_bounds__(kPcgKxThreads)
     const int le = lane < 27 ? lane : lane - 27;  // lanes 27..31 shadow lanes 0..4 and never write
     const int sub = le / 9, col = le - sub * 9;
     const int ci = col / 3, cj = col - ci * 3;
-    const int wcx = warp >> 2, wcy = ((warp & 3) - wcx) & 3;  // one column of every cx and cy per scheduler
-    const int cb = wcx * 16 + wcy * 4;
+    // column h of warp w: index w + 8 h, cx its high bits, cy rotated by cx
+    // (the warps of a scheduler hold one column of every cx and cy)
+    int cpos[kPcgKxCols], cb[kPcgKxCols];
+#pragma unroll
+    for (int h = 0; h < kPcgKxCols; ++h) {
+        const int cidx = warp + h * kPcgKxWarps;
+        const int cx = cidx >> 2, cy = ((cidx & 3) - cx) & 3;
+        cpos[h] = cx * 4 + cy;
+        cb[h] = cx * 16 + cy * 4;
+    }
     KxPiece px, py;
     px.init(ci, inv_dx);
     py.init(cj, inv_dx);
@@ -256,7 +266,11 @@ __global__ void __launch_bounds__(kPcgKxThreads)
         int bx, by, bz;
         page_coords(bin.block_keys[b], bx, by, bz);
         __syncthreads();
-        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double acc[kPcgKxCols][6];
+#pragma unroll
+        for (int h = 0; h < kPcgKxCols; ++h)
+#pragma unroll
+            for (int z = 0; z < 6; ++z) acc[h][z] = 0.0;
         for (int c0 = cstart[0]; c0 < cstart[64]; c0 += kPcgKxChunk) {
             const int c1 = min(cstart[64], c0 + kPcgKxChunk);
             __syncthreads();
@@ -275,23 +289,30 @@ __global__ void __launch_bounds__(kPcgKxThreads)
                 for (int a = 0; a < 3; ++a) r[8 + a] = P.col[(int64_t)a * P.n + slot];
             }
             __syncthreads();
-            kx_cell<0>(recs, cstart, cb, c0, c1, sub, px, py, inv_dx, acc);
-            kx_cell<1>(recs, cstart, cb, c0, c1, sub, px, py, inv_dx, acc);
-            kx_cell<2>(recs, cstart, cb, c0, c1, sub, px, py, inv_dx, acc);
-            kx_cell<3>(recs, cstart, cb, c0, c1, sub, px, py, inv_dx, acc);
+#pragma unroll
+            for (int h = 0; h < kPcgKxCols; ++h) {
+                kx_cell<0>(recs, cstart, cb[h], c0, c1, sub, px, py, inv_dx, acc[h]);
+                kx_cell<1>(recs, cstart, cb[h], c0, c1, sub, px, py, inv_dx, acc[h]);
+                kx_cell<2>(recs, cstart, cb[h], c0, c1, sub, px, py, inv_dx, acc[h]);
+                kx_cell<3>(recs, cstart, cb[h], c0, c1, sub, px, py, inv_dx, acc[h]);
+            }
         }
         // the three particle streams of a stencil column, in fixed order
 #pragma unroll
-        for (int z = 0; z < 6; ++z) {
-            const double v1 = __shfl_sync(0xffffffffu, acc[z], (lane + 9) & 31);
-            const double v2 = __shfl_sync(0xffffffffu, acc[z], (lane + 18) & 31);
-            acc[z] = (acc[z] + v1) + v2;
-        }
+        for (int h = 0; h < kPcgKxCols; ++h)
+#pragma unroll
+            for (int z = 0; z < 6; ++z) {
+                const double v1 = __shfl_sync(0xffffffffu, acc[h][z], (lane + 9) & 31);
+                const double v2 = __shfl_sync(0xffffffffu, acc[h][z], (lane + 18) & 31);
+                acc[h][z] = (acc[h][z] + v1) + v2;
+            }
         __syncthreads();  // every warp is past its sweep: the staging buffer is free
         double* colsum = recs;  // [column 4 cx + cy][stencil column][z]
         if (lane < 9) {
 #pragma unroll
-            for (int z = 0; z < 6; ++z) colsum[((wcx * 4 + wcy) * 9 + col) * 6 + z] = acc[z];
+            for (int h = 0; h < kPcgKxCols; ++h)
+#pragma unroll
+                for (int z = 0; z < 6; ++z) colsum[(cpos[h] * 9 + col) * 6 + z] = acc[h][z];
         }
         __syncthreads();
         if (t < kWindowNodes) {
@@ -464,7 +485,7 @@ cudaError_t launch_pcg_iteration(const SceneDev<R>* sc, const PState<R>& st, con
     const int pages = max(1, min(bin.nb_cap, cfg.num_sms * 4));
     const int gb = pcg_grid_blocks(bin, cfg);
     k_pcg_col<R><<<pages, kPcgColThreads, 0, stream>>>(sc, st, aux, bin, P, cnt);
-    k_pcg_kx<R><<<pages, kPcgKxThreads, 0, stream>>>(sc, st, bin, P, tile, cnt);
+    k_pcg_kx<R><<<max(1, min(bin.nb_cap, cfg.num_sms * 8)), kPcgKxThreads, 0, stream>>>(sc, st, bin, P, tile, cnt);
     k_pcg_q<<<gb, kPcgBlock, 0, stream>>>(bin, P, tile, cnt, cfg.pcg_mobility);
     k_pcg_alpha<<<1, kPcgScalarThreads, 0, stream>>>(P, bin, cnt, cfg.pcg_max_combine);
     k_pcg_update<<<gb, kPcgBlock, 0, stream>>>(bin, P, cnt);
