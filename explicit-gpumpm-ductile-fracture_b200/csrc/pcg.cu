@@ -140,7 +140,52 @@ __global__ void __launch_bounds__(kPcgColThreads)
     __shared__ double win[kWindowNodes];
     const int nb = min(cnt->n_blocks, bin.nb_cap);
     const double dx = sc->dx_d, inv_dx = sc->inv_dx_d;
+    // col of the particle in `slot` (previous slot o, cell, position x, volume, id)
+    auto particle = [&](int slot, int o, uint32_t cell, const R* x, R vol, uint32_t idw, int bx, int by, int bz) {
+        const int li = (int)(cell >> 4), lj = (int)((cell >> 2) & 3), lk = (int)(cell & 3);
+        const double xp[3] = {(double)x[0] - (double)(4 * bx + li) * dx, (double)x[1] - (double)(4 * by + lj) * dx,
+                              (double)x[2] - (double)(4 * bz + lk) * dx};
+        double w[3][3], gr[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) bspline_k(xp[a], inv_dx, k, w[a][k], gr[a][k]);
+        double col[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const double xn = win[(li + i) * 36 + (lj + j) * 6 + (lk + k)];
+                    col[0] += gr[0][i] * w[1][j] * w[2][k] * xn;
+                    col[1] += w[0][i] * gr[1][j] * w[2][k] * xn;
+                    col[2] += w[0][i] * w[1][j] * gr[2][k] * xn;
+                }
+        const double L0 = (double)sc->mat[idw >> 28].length_scale;
+        const double para = (double)vol * 4.0 * L0 * L0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) P.col[(int64_t)a * P.n + slot] = col[a] * para;
+        (void)o;
+    };
     for (int b = blockIdx.x; b < nb; b += gridDim.x) {
+        // The page's bounds and this thread's first particle are loaded before
+        // the window, so the two chains of dependent loads overlap.
+        const int s0 = bin.cell_start[(int64_t)b * 64], s1 = bin.cell_start[(int64_t)b * 64 + 64];
+        int bx, by, bz;
+        page_coords(bin.block_keys[b], bx, by, bz);
+        const int slot0 = s0 + (int)threadIdx.x;
+        int o0 = 0;
+        uint32_t cell0 = 0, id0 = 0;
+        R x0[3] = {R(0), R(0), R(0)}, vol0 = R(0);
+        if (slot0 < s1) {
+            o0 = bin.perm[slot0];
+            cell0 = bin.keys_sorted[slot0] & 63u;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) x0[a] = st.x[a][o0];
+            vol0 = aux.vol[o0];
+            id0 = st.id[o0];
+        }
         __syncthreads();
         for (int w = threadIdx.x; w < kWindowNodes; w += kPcgColThreads) {
             const int a = w / 36, bb = (w / 6) % 6, cc = w % 6;
@@ -149,37 +194,11 @@ __global__ void __launch_bounds__(kPcgColThreads)
             win[w] = g < 0 ? 0.0 : P.s[(int64_t)g * 64 + (a & 3) * 16 + (bb & 3) * 4 + (cc & 3)];
         }
         __syncthreads();
-        int bx, by, bz;
-        page_coords(bin.block_keys[b], bx, by, bz);
-        const int s0 = bin.cell_start[(int64_t)b * 64], s1 = bin.cell_start[(int64_t)b * 64 + 64];
-        for (int slot = s0 + threadIdx.x; slot < s1; slot += kPcgColThreads) {
+        if (slot0 < s1) particle(slot0, o0, cell0, x0, vol0, id0, bx, by, bz);
+        for (int slot = slot0 + kPcgColThreads; slot < s1; slot += kPcgColThreads) {
             const int o = bin.perm[slot];
-            const uint32_t cell = bin.keys_sorted[slot] & 63u;
-            const int li = (int)(cell >> 4), lj = (int)((cell >> 2) & 3), lk = (int)(cell & 3);
-            const double xp[3] = {(double)st.x[0][o] - (double)(4 * bx + li) * dx,
-                                  (double)st.x[1][o] - (double)(4 * by + lj) * dx,
-                                  (double)st.x[2][o] - (double)(4 * bz + lk) * dx};
-            double w[3][3], gr[3][3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) bspline_k(xp[a], inv_dx, k, w[a][k], gr[a][k]);
-            double col[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const double xn = win[(li + i) * 36 + (lj + j) * 6 + (lk + k)];
-                        col[0] += gr[0][i] * w[1][j] * w[2][k] * xn;
-                        col[1] += w[0][i] * gr[1][j] * w[2][k] * xn;
-                        col[2] += w[0][i] * w[1][j] * gr[2][k] * xn;
-                    }
-            const double L0 = (double)sc->mat[st.id[o] >> 28].length_scale;
-            const double para = (double)aux.vol[o] * 4.0 * L0 * L0;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) P.col[(int64_t)a * P.n + slot] = col[a] * para;
+            const R x[3] = {st.x[0][o], st.x[1][o], st.x[2][o]};
+            particle(slot, o, bin.keys_sorted[slot] & 63u, x, aux.vol[o], st.id[o], bx, by, bz);
         }
     }
 }
