@@ -155,6 +155,7 @@ void fill_scene_dev(const gmpm_scene_desc& d, int key_bits, SceneDev<R>& s) {
         o.yield_stress = (R)in.yield_stress;
         o.hardening = (R)in.hardening;
         o.hardening_law = in.hardening_law;
+        o.energy_model = in.energy_model;
         o.alpha_cap = (R)in.alpha_cap;
         o.dlambda_cap = (R)in.dlambda_cap;
         o.strain_cap = (R)in.strain_cap;
@@ -208,6 +209,8 @@ gmpm_status validate(const gmpm_scene_desc* d, const gmpm_particle_init* init) {
         if (!(mt.youngs_modulus > 0) || !(mt.poisson_ratio >= 0) || !(mt.poisson_ratio < 0.5)) return GMPM_INVALID_ARG;
         if (!(mt.fracture_energy > 0)) return GMPM_INVALID_ARG;
         if (mt.hardening_law != GMPM_HARDENING_EXPONENTIAL && mt.hardening_law != GMPM_HARDENING_LINEAR)
+            return GMPM_INVALID_ARG;
+        if (mt.energy_model < GMPM_ENERGY_VON_MISES_FRACTURE || mt.energy_model > GMPM_ENERGY_NEO_HOOKEAN_FRACTURE)
             return GMPM_INVALID_ARG;
     }
     if (d->n_slab_bcs < 0 || d->n_slab_bcs > GMPM_MAX_SLAB_BCS) return GMPM_INVALID_ARG;
@@ -316,8 +319,10 @@ struct Scene : SceneBase {
     }
 
     LaunchCfg cfg() const {
+        int other = 0;
+        for (int m = 0; m < desc.n_materials; ++m) other |= desc.materials[m].energy_model != GMPM_ENERGY_VON_MISES_FRACTURE;
         return LaunchCfg{share_ > 0 ? std::min(share_, ctx->num_sms) : ctx->num_sms, desc.deterministic,
-                         desc.pcg_max_combine, desc.materials[0].mobility, desc.pcg_tolerance};
+                         desc.pcg_max_combine, desc.materials[0].mobility, desc.pcg_tolerance, other};
     }
     bool implicit_pf() const { return desc.phase_field == GMPM_PHASE_FIELD_IMPLICIT; }
     int* pcg_done_host = nullptr;  // pinned: the solve's done flag, read between iterations

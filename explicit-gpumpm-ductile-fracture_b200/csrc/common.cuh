@@ -39,6 +39,7 @@ struct MaterialDev {
     Real D[9];              // inverse of the isotropic stiffness (Gauss-Jordan as in Inverse())
     Real yield_stress, hardening;
     int hardening_law;
+    int energy_model;       // gmpm_energy_model
     Real alpha_cap, dlambda_cap, strain_cap, psi_cap;
     Real fracture_energy, softening_onset, residual_fracture;
     Real theta, length_scale, mobility;

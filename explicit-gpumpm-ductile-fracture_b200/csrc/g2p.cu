@@ -195,7 +195,7 @@ __device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int 
     }
 }
 
-template <typename R>
+template <typename R, bool kAnyModel>
 __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
     k_g2p(const SceneDev<R>* __restrict__ sc, const SceneDev<double>* __restrict__ sc64, PState<R> in,
           PState<R> out, PAux<R> aux, BinDev bin, const R* __restrict__ nodes, Counters* cnt) {
@@ -402,14 +402,14 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
             const R g_old = c_old * c_old * (R(1) - theta) + theta;
             const R alpha_in = S.p[buf][P_ALPHA][t], psi_in = S.p[buf][P_PSI][t];
             StressOut<R> so;
-            von_mises_update<R, R>(M, V0, Fo, g_old, alpha_in, c_new, psi_in, so);
+            constitutive_update<R, R, kAnyModel>(M, V0, dx, Fo, g_old, alpha_in, c_new, psi_in, so);
             if (fallback && so.smin_over_smax < ratio) {
                 // FP64 SVD + return map for ill-conditioned F
                 double Fd[9];
 #pragma unroll
                 for (int q = 0; q < 9; ++q) Fd[q] = (double)Fo[q];
                 StressOut<double> sd;
-                von_mises_update<double, double>(sc64->mat[mat], (double)V0, Fd, (double)g_old, (double)alpha_in,
+                constitutive_update<double, double, kAnyModel>(sc64->mat[mat], (double)V0, sc64->dx, Fd, (double)g_old, (double)alpha_in,
                                                  (double)c_new, (double)psi_in, sd);
 #pragma unroll
                 for (int q = 0; q < 9; ++q) so.F[q] = (R)sd.F[q];
@@ -469,7 +469,10 @@ __global__ void k_advance_time(Counters* cnt, SceneDev<R>* sc, SceneDev<double>*
 
 template <typename R>
 cudaError_t prepare_g2p() {
-    return cudaFuncSetAttribute(k_g2p<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(G2PShared<R>));
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_g2p<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(G2PShared<R>));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_g2p<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(G2PShared<R>));
 }
 template cudaError_t prepare_g2p<float>();
 template cudaError_t prepare_g2p<double>();
@@ -481,7 +484,11 @@ cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, cons
     const int per_sm = sizeof(R) == 4 ? kG2PMinBlocks : 1;
     const int64_t units = (bin.n + kG2PUnit - 1) / kG2PUnit;
     const int ctas = (int)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)cfg.num_sms * per_sm));
-    k_g2p<R><<<ctas, kG2PUnit, sizeof(G2PShared<R>), stream>>>(sc, fallback64, in, out, aux, bin,
+    if (cfg.other_models)
+        k_g2p<R, true><<<ctas, kG2PUnit, sizeof(G2PShared<R>), stream>>>(sc, fallback64, in, out, aux, bin,
+                                               reinterpret_cast<const R*>(grid.nodes), cnt);
+    else
+        k_g2p<R, false><<<ctas, kG2PUnit, sizeof(G2PShared<R>), stream>>>(sc, fallback64, in, out, aux, bin,
                                                reinterpret_cast<const R*>(grid.nodes), cnt);
     k_advance_time<R><<<1, 1, 0, stream>>>(cnt, const_cast<SceneDev<R>*>(sc), const_cast<SceneDev<double>*>(sc64));
     return cudaGetLastError();

@@ -48,6 +48,7 @@ struct LaunchCfg {
     int pcg_max_combine;   // implicit phase field settings
     double pcg_mobility;
     double pcg_tolerance;
+    int other_models;      // a material uses an energy model other than von Mises
 };
 
 template <typename R>

@@ -7,7 +7,8 @@
 
 namespace gmpm {
 
-// The reference's first applyVonMises runs at the start of substep 1 with the
+// The reference's first applyVonMises (or its other energy models' contribution
+// kernels) runs at the start of substep 1 with the
 // initial state g = 1 (initArray, Particle_kernal.cu:451-454); here it runs at
 // scene creation so every substep can start at P2G.
 template <typename R>
@@ -20,7 +21,7 @@ __global__ void k_init_stress(const SceneDev<R>* __restrict__ sc, PState<R> st, 
     for (int q = 0; q < 9; ++q) F[q] = st.F[q][p];
     const int mat = (int)(st.id[p] >> 28);
     StressOut<R> so;
-    von_mises_update<R, R>(sc->mat[mat], sc->V0, F, R(1), st.alpha[p], st.c[p], st.psi[p], so);
+    constitutive_update<R, R>(sc->mat[mat], sc->V0, sc->dx, F, R(1), st.alpha[p], st.c[p], st.psi[p], so);
     if (!so.svd_ok) raise_flag(cnt, GMPM_FLAG_SVD_NOCONVERGE);
 #pragma unroll
     for (int q = 0; q < 9; ++q) {

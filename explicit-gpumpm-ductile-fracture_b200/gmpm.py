@@ -32,6 +32,7 @@ FIELD = dict(position=0, velocity=1, F=2, B=3, damage=4, alpha=5, psi_max=6, str
              pf_flux=10, mass=11, id=12)
 FIELD_COMPONENTS = dict(position=3, velocity=3, F=9, B=9, damage=1, alpha=1, psi_max=1, stress=6, volume=1, FP=1,
                         pf_flux=3, mass=1, id=1)
+ENERGY_VON_MISES_FRACTURE, ENERGY_FIXED_COROTATED, ENERGY_NEO_HOOKEAN_FRACTURE = 0, 1, 2
 DTYPE_F64, DTYPE_F32, DTYPE_I32 = 0, 1, 2
 ORDER_INTERNAL, ORDER_ORIGINAL = 0, 1
 BIN = dict(counts=0, perm=1, keys=2, block_keys=3, block_start=4, cell_start=5, grid_keys=6, adj=7)
@@ -41,7 +42,7 @@ NOALLOC_MAX_RES = 128
 
 class Material(C.Structure):
     _fields_ = [("youngs_modulus", C.c_double), ("poisson_ratio", C.c_double), ("density", C.c_double),
-                ("yield_stress", C.c_double), ("hardening_law", C.c_int32), ("_pad0", C.c_int32),
+                ("yield_stress", C.c_double), ("hardening_law", C.c_int32), ("energy_model", C.c_int32),
                 ("hardening", C.c_double), ("alpha_cap", C.c_double), ("dlambda_cap", C.c_double),
                 ("strain_cap", C.c_double), ("psi_cap", C.c_double), ("fracture_energy", C.c_double),
                 ("softening_onset", C.c_double), ("residual_fracture", C.c_double), ("theta", C.c_double),

@@ -64,6 +64,19 @@ typedef enum gmpm_hardening {
     GMPM_HARDENING_LINEAR = 1         /* R(alpha) = yield + H * alpha */
 } gmpm_hardening;
 
+/* Energy model of a material: the reference's compile-time Energy_Model
+ * (Setting.h:38), selectable per material here. */
+typedef enum gmpm_energy_model {
+    GMPM_ENERGY_VON_MISES_FRACTURE = 0,  /* Energy_Model 2: Hencky von Mises plasticity with hardening and
+                                            phase-field fracture (applyVonMises,
+                                            ExplicitTimeIntegrator.cu:132-370) */
+    GMPM_ENERGY_FIXED_COROTATED = 1,     /* Energy_Model 0: elastic fixed-corotated, no fracture driving
+                                            (computeContributionFixedCorotated, :22-47) */
+    GMPM_ENERGY_NEO_HOOKEAN_FRACTURE = 2 /* Energy_Model 1: elastic Neo-Hookean with the tension/compression
+                                            split and phase-field fracture driving; G_c = 3 and L0 = dx/2 as
+                                            hard-coded there (computeContributionNeoHookean, :372-446) */
+} gmpm_energy_model;
+
 typedef enum gmpm_phase_field {
     GMPM_PHASE_FIELD_OFF = 0,
     GMPM_PHASE_FIELD_EXPLICIT = 1,    /* explicit diffusion, pointwise-implicit reaction */
@@ -81,7 +94,7 @@ typedef struct gmpm_material {
     double density;            /* rho (informational; particle masses are explicit) */
     double yield_stress;       /* reference 800 */
     int32_t hardening_law;     /* gmpm_hardening */
-    int32_t _pad0;
+    int32_t energy_model;      /* gmpm_energy_model; 0 (von Mises with fracture) by default */
     double hardening;          /* exponential rate h (reference 3) or linear modulus H */
     double alpha_cap;          /* alpha_c, reference 1 */
     double dlambda_cap;        /* reference 100 */

@@ -644,6 +644,105 @@ void von_mises(const MatConsts& mc, double V0, const double* Fin, double g, doub
     o.vol = V0 * det;
 }
 
+// P = U diag(Ph) V^T and contribution(r,c) = V0 * sum_k P(r,k) F(c,k), as the
+// reference's contribution kernels (ExplicitTimeIntegrator.cu:41-46, :440-445).
+// U and V column-major.
+static void elastic_contribution(const double* U, const double* V, const double* Ph, const double* F, double V0,
+                                 double* contrib) {
+    double P[9];
+    for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc)
+            P[r + 3 * cc] = Ph[0] * U[r] * V[cc] + Ph[1] * U[r + 3] * V[cc + 3] + Ph[2] * U[r + 6] * V[cc + 6];
+    for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc)
+            contrib[r + 3 * cc] = (P[r] * F[cc] + P[r + 3] * F[cc + 3] + P[r + 6] * F[cc + 6]) * V0;
+}
+
+static void svd_colmajor(const double* F, double* U, double* S, double* V) {
+    M3 A, Um, Vm;
+    for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc) A(r, cc) = F[r + 3 * cc];
+    qr_svd(A, S, Um, Vm);
+    for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc) {
+            U[r + 3 * cc] = Um(r, cc);
+            V[r + 3 * cc] = Vm(r, cc);
+        }
+}
+
+static double det_colmajor(const double* F) {
+    return F[0] * F[4] * F[8] + F[3] * F[7] * F[2] + F[6] * F[1] * F[5] - F[2] * F[4] * F[6] - F[1] * F[3] * F[8] -
+           F[0] * F[5] * F[7];
+}
+
+// computeContributionFixedCorotated (ExplicitTimeIntegrator.cu:22-47): elastic,
+// no fracture driving (FP = 1); F, alpha, psi and g unchanged.
+void fixed_corotated(const MatConsts& mc, double V0, const double* F, double g, double alpha, double psi, VMOut& o) {
+    double U[9], V[9], S[3];
+    svd_colmajor(F, U, S, V);
+    const double J = S[0] * S[1] * S[2];
+    const double smu = 2.0 * mc.mu, slam = mc.lambda * (J - 1.0);
+    const double Ph[3] = {smu * (S[0] - 1.0) + slam * (S[1] * S[2]), smu * (S[1] - 1.0) + slam * (S[0] * S[2]),
+                          smu * (S[2] - 1.0) + slam * (S[0] * S[1])};
+    elastic_contribution(U, V, Ph, F, V0, o.contrib);
+    for (int i = 0; i < 9; ++i) o.F[i] = F[i];
+    o.g = g;
+    o.alpha = alpha;
+    o.psi = psi;
+    o.FP = 1.0;
+    o.vol = V0 * det_colmajor(F);
+}
+
+// computeContributionNeoHookean (ExplicitTimeIntegrator.cu:372-446): elastic
+// Neo-Hookean with the tension/compression split; psi+ history (cap 1e6),
+// FP = 4 L0 (1 - 0.001f) psi / G_c + 1 with G_c = 3 and L0 = dx/2, and
+// g = c^2 (1 - 1e-4f) + 1e-4f.  J^(-2/3) is the reference's single-precision
+// power, taken here as the correctly rounded float value of the double power.
+void neo_hookean_fracture(const MatConsts& mc, double V0, double dx, const double* F, double alpha, double c,
+                          double psi, VMOut& o) {
+    double U[9], V[9], S[3];
+    svd_colmajor(F, U, S, V);
+    const double mu = mc.mu, kappa = mc.kappa;
+    const double J = S[0] * S[1] * S[2];
+    const double Jbar = (double)(float)std::pow((double)(float)J, (double)(-2.0f / 3.0f));
+    double bb[3];
+    for (int k = 0; k < 3; ++k) bb[k] = Jbar * S[k] * S[k];
+    const double bbs = bb[0] + bb[1] + bb[2];
+    const double lnJ = std::log(J);
+    const double psi_vol = kappa / 2.0 * ((J - 1.0) / 2.0 - lnJ);
+    const double psi_dev = mu / 2.0 * (bb[0] + bb[1] + bb[2] - 3.0);
+    const double psi_pos = (J < 1.0) ? psi_dev : psi_dev + psi_vol;
+    if (psi_pos > psi && psi_pos < 1e6) psi = psi_pos;
+    const double L0 = 0.5 * dx;
+    const double FP = 4.0 * L0 * (double)(1.f - 0.001f) * psi * 1.0 / 3.0 + 1.0;
+    const double tvol = kappa / 2.0 * (J * J - 1.0);
+    const double third = (double)(1.f / 3.f) * bbs;
+    const double gn = c * c * (double)(1.f - 0.0001f) + (double)0.0001f;
+    double Ph[3];
+    for (int k = 0; k < 3; ++k) {
+        const double td = mu * (bb[k] - third);
+        Ph[k] = (J < 1.0) ? gn * td + tvol : gn * (td + tvol);
+    }
+    elastic_contribution(U, V, Ph, F, V0, o.contrib);
+    for (int i = 0; i < 9; ++i) o.F[i] = F[i];
+    o.g = gn;
+    o.alpha = alpha;
+    o.psi = psi;
+    o.FP = FP;
+    o.vol = V0 * det_colmajor(F);
+}
+
+// The material's energy model (gmpm_material::energy_model).
+void constitutive(const MatConsts& mc, double V0, double dx, const double* F, double g, double alpha, double c,
+                  double psi, VMOut& o) {
+    if (mc.m->energy_model == GMPM_ENERGY_FIXED_COROTATED)
+        fixed_corotated(mc, V0, F, g, alpha, psi, o);
+    else if (mc.m->energy_model == GMPM_ENERGY_NEO_HOOKEAN_FRACTURE)
+        neo_hookean_fracture(mc, V0, dx, F, alpha, c, psi, o);
+    else
+        von_mises(mc, V0, F, g, alpha, c, psi, o);
+}
+
 // ---------------------------------------------------------------------------
 // Quadratic B-spline weights (P2GKernal.cu:590-611, G2PKernal.cu:263-287).
 // ---------------------------------------------------------------------------
@@ -1146,7 +1245,7 @@ void grid_update(orc_scene& s) {
 void stress_one(orc_scene& s, int64_t p) {
     const MatConsts& mc = s.mc[s.mat[p]];
     VMOut o;
-    von_mises(mc, s.desc.particle_volume, &s.F[9 * p], s.g[p], s.alpha[p], s.c[p], s.psi[p], o);
+    constitutive(mc, s.desc.particle_volume, s.desc.dx, &s.F[9 * p], s.g[p], s.alpha[p], s.c[p], s.psi[p], o);
     for (int q = 0; q < 9; ++q) {
         s.F[9 * p + q] = o.F[q];
         s.sigma[9 * p + q] = o.contrib[q];
