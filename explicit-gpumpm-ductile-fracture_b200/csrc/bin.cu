@@ -208,9 +208,33 @@ __device__ __forceinline__ void canon_rank(const BinDev& bin, const int32_t* cs,
     }
 }
 
+// Warp path: the scatter keeps the order of the lanes of one warp, so most
+// cells already ascend by previous slot.  Only the cells with a descent are
+// ranked; an ascending cell is its own canonical order.
+__device__ __forceinline__ void canon_rank_warp(const BinDev& bin, const int32_t* cs, const int32_t* buf,
+                                                uint8_t* bad, int lo, int hi, int lane) {
+    for (int c = lane; c < 64; c += 32) bad[c] = 0;
+    __syncwarp();
+    for (int s = lo + lane; s < hi; s += 32) {
+        const int cell = (int)(bin.keys_sorted[s] & 63);
+        if (s > cs[cell] && buf[s - lo - 1] > buf[s - lo]) bad[cell] = 1;
+    }
+    __syncwarp();
+    for (int s = lo + lane; s < hi; s += 32) {
+        const int cell = (int)(bin.keys_sorted[s] & 63);
+        if (!bad[cell]) continue;
+        const int a = cs[cell] - lo, e = cs[cell + 1] - lo;
+        const int32_t v = buf[s - lo];
+        int r = 0;
+        for (int u = a; u < e; ++u) r += buf[u] < v;
+        bin.perm[lo + a + r] = v;
+    }
+}
+
 __global__ void __launch_bounds__(32 * kCanonWarps) k_bin_canon(BinDev bin, Counters* cnt) {
     __shared__ int32_t buf[kCanonBuf];
     __shared__ int32_t cs[kCanonWarps][68];
+    __shared__ uint8_t bad[kCanonWarps][64];
     __shared__ int big[kCanonWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nb = min(cnt->n_blocks, bin.nb_cap);
@@ -225,7 +249,7 @@ __global__ void __launch_bounds__(32 * kCanonWarps) k_bin_canon(BinDev bin, Coun
             if (hi - lo <= kCanonWarpBuf) {
                 for (int s = lo + lane; s < hi; s += 32) wbuf[s - lo] = bin.perm[s];
                 __syncwarp();
-                canon_rank(bin, cs[warp], wbuf, lo, hi, lane, 32);
+                canon_rank_warp(bin, cs[warp], wbuf, bad[warp], lo, hi, lane);
             } else {
                 is_big = 1;
             }
