@@ -19,9 +19,9 @@
 // that the reference runs at the start of substep n+1 is run at the end of
 // G2P of substep n (it reads only G2P's outputs), plus once at scene creation.
 //
-// Phase field: the north star replaces the reference's implicit Jacobi-PCG
-// solve (ExplicitTimeIntegrator.cu:909-972) with an explicit update of the
-// same discrete operator (lumped mass M_L = sum V w, reaction diagonal
+// Phase field: the default (explicit) mode replaces the reference's implicit
+// Jacobi-PCG solve (ExplicitTimeIntegrator.cu:909-972) with an explicit update
+// of the same discrete operator (lumped mass M_L = sum V w, reaction diagonal
 // sum V w (1/dt + M FP), stiffness K = sum 4 L0^2 V grad w grad w^T):
 //     c_new_i = (M_L,i (c_i/dt + M) - M (K c~)_i) / (M_L,i/dt + M sum V w FP)
 // where (K c~)_i = sum_p grad w_ip . q_p and q_p = 4 L0^2 V_p grad c_p, with
