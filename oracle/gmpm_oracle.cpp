@@ -1366,6 +1366,20 @@ void orc_von_mises(const gmpm_material* mat, double V0, const double* io, double
     out[22] = o.vol;
 }
 
+void orc_constitutive(const gmpm_material* mat, double V0, double dx, const double* io, double* out) {
+    MatConsts mc;
+    mc.init(mat);
+    VMOut o;
+    constitutive(mc, V0, dx, io, io[9], io[10], io[11], io[12], o);
+    for (int q = 0; q < 9; ++q) out[q] = o.F[q];
+    out[9] = o.g;
+    out[10] = o.alpha;
+    out[11] = o.psi;
+    out[12] = o.FP;
+    for (int q = 0; q < 9; ++q) out[13 + q] = o.contrib[q];
+    out[22] = o.vol;
+}
+
 void orc_set_threads(int n) {
     g_threads = n;
 #ifdef _OPENMP

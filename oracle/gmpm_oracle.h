@@ -43,6 +43,11 @@ void orc_lame(double E, double nu, double* lambda, double* mu, double* kappa);
  *      [13..21] contribution V0*P*F^T col-major, [22] V0*det F. */
 void orc_von_mises(const gmpm_material* mat, double V0, const double* io, double* out);
 
+/* The same update through the material's energy model (mat->energy_model:
+ * von Mises, fixed-corotated or Neo-Hookean with fracture); dx sets the
+ * Neo-Hookean phase-field length L0 = dx/2.  Same io / out layout. */
+void orc_constitutive(const gmpm_material* mat, double V0, double dx, const double* io, double* out);
+
 typedef struct orc_scene orc_scene;
 
 orc_scene* orc_scene_create(const gmpm_scene_desc* desc, int64_t n, const double* pos,

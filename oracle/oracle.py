@@ -44,6 +44,7 @@ def lib(desc_type=None, diag_type=None, material_type=None) -> C.CDLL:
         L.orc_svd3.argtypes = [dp, dp, dp, dp]
         L.orc_lame.argtypes = [C.c_double, C.c_double, dp, dp, dp]
         L.orc_von_mises.argtypes = [vp, C.c_double, dp, dp]
+        L.orc_constitutive.argtypes = [vp, C.c_double, C.c_double, dp, dp]
         L.orc_scene_create.restype = vp
         L.orc_scene_create.argtypes = [vp, C.c_int64, dp, dp, dp, ip]
         L.orc_scene_destroy.argtypes = [vp]
