@@ -397,7 +397,34 @@ def run_served(pkg, local_rank: int, duration_s: float) -> dict:
     r = serving.run_served(ctx, duration_s=duration_s, rate_hz=20.0, seed=0, stream=stream.cuda_stream)
     r["workload"] = ("Poisson 20 req/s, notched bar or plate impact 50/50, 20k-2M particles log-uniform, "
                      "horizons U[200,2000] substeps, params +/-50%, 120 GB budget, FP32 + FP64 SVD fallback")
+    plain = served_plain_sequential(pkg, ctx, stream)
+    r["plain_sequential"] = plain
+    r["speedup_vs_plain"] = r["particle_substeps_per_s"] / plain["value"]
     return r
+
+
+def served_plain_sequential(pkg, ctx, stream, n_requests: int = 32, substeps: int = 10, seed: int = 0) -> dict:
+    """The first requests of the served workload's generator, one at a time
+    through the plain path: each scene alone for a fixed number of substeps,
+    CUDA events around each scene's substeps, summed."""
+    import torch
+
+    prng = np.random.default_rng(seed + 1)  # the served run's request generator
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    work, ms = 0, 0.0
+    for k in range(n_requests):
+        sp, _ = pkg.scenes.served_request(prng, k)
+        sc = sp.build(ctx)
+        sc.substep(2, stream.cuda_stream)
+        e0.record(stream)
+        sc.substep(substeps, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        work += sp.n * substeps
+        sc.close()
+    return dict(value=work / (ms / 1e3), requests=n_requests, substeps_each=substeps,
+                particles=int(work // substeps))
 
 
 def sizeof_velocity_conditions(dt) -> int:
