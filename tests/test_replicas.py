@@ -5,6 +5,7 @@ of bench.py as two gloo ranks on the CPU."""
 from __future__ import annotations
 
 import importlib.util
+import json
 import os
 import socket
 import subprocess
@@ -75,3 +76,24 @@ def test_reference_arm_runs_on_rank_zero_only():
                        cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_line_contract():
+    """Rank 0's reference line: the same metric, unit and workload as the
+    CUDA arm, at least 3 warm-up steps, impl "reference", and cpu_baseline
+    and e2e objects that repeat the line's own value with no transfers."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["metric"] == "particle-substeps/sec" and line["unit"] == "particle-substeps/s"
+    assert line["higher_is_better"] is True and line["value"] > 0
+    assert line["warmup"] >= 3 and line["steps"] == 1
+    assert line["config"]["workload"].startswith("plates_33m: 4 plates of 256x256x16 cells")
+    cpu, e2e = line["cpu_baseline"], line["e2e"]
+    assert cpu["value"] == line["value"] and cpu["kind"] in ("port", "reference") and cpu["cores"] >= 1
+    assert cpu["sample"]
+    assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
