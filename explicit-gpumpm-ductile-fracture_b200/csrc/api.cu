@@ -36,7 +36,7 @@ std::atomic<uint64_t> g_scene_uid{1};
 // Checkpoint file: this header, the scene description, then every particle
 // plane of the state (n values each, in the internal order).
 constexpr char kSnapshotMagic[8] = {'G', 'M', 'P', 'M', 'S', 'N', 'A', 'P'};
-constexpr uint32_t kSnapshotVersion = 1;
+constexpr uint32_t kSnapshotVersion = 2;  // 2: F and the plastic state as four-wide words
 struct SnapshotHeader {
     char magic[8];
     uint32_t version;
@@ -361,8 +361,9 @@ struct Scene : SceneBase {
         GMPM_TRY(alloc(&grid.diag, 8));
         GMPM_TRY(cudaMemset(grid.diag, 0, 8 * sizeof(double)));
 
-        // particle planes: 2 x (x3 F9 c alpha psi m) + aux (v3 B9 sigma6 vol FP q3), + 2 id planes
-        const int state_planes = 16, aux_planes = 23;
+        // particle planes: 2 x (x3 c m + 3 four-wide words F/alpha/psi) + aux (v3 B9 sigma6 vol FP q3),
+        // + 2 id planes
+        const int state_planes = 5 + 3 * 4, aux_planes = 23;
         const size_t nplanes = 2 * state_planes + aux_planes;
         const size_t plane_bytes = round_up((size_t)stride * sizeof(R), 256);
         const size_t id_bytes = round_up((size_t)stride * sizeof(uint32_t), 256);
@@ -375,13 +376,16 @@ struct Scene : SceneBase {
             base += plane_bytes;
             return p;
         };
+        auto next_word = [&]() {
+            Word4<R>* p = reinterpret_cast<Word4<R>*>(base);
+            base += 4 * plane_bytes;
+            return p;
+        };
         for (int b = 0; b < 2; ++b) {
             st[b].stride = stride;
             for (int a = 0; a < 3; ++a) st[b].x[a] = next();
-            for (int q = 0; q < 9; ++q) st[b].F[q] = next();
+            for (int k = 0; k < 3; ++k) st[b].fw[k] = next_word();
             st[b].c = next();
-            st[b].alpha = next();
-            st[b].psi = next();
             st[b].m = next();
         }
         for (int a = 0; a < 3; ++a) aux.v[a] = next();
@@ -406,15 +410,15 @@ struct Scene : SceneBase {
             }
             for (int64_t p = 0; p < n; ++p) tmp[p] = (R)init->masses[p];
             GMPM_TRY(cudaMemcpy(st[0].m, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
-            for (int q = 0; q < 9; ++q) {
-                const R v = (q % 4 == 0) ? R(1) : R(0);
-                for (int64_t p = 0; p < n; ++p) tmp[p] = v;
-                GMPM_TRY(cudaMemcpy(st[0].F[q], tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
+            {
+                // F = I (F0, F4 and F8 are the diagonal), alpha = psi_max = 0
+                const Word4<R> w{{R(1), R(0), R(0), R(0)}};
+                std::vector<Word4<R>> words((size_t)n, w);
+                for (int k = 0; k < 3; ++k)
+                    GMPM_TRY(cudaMemcpy(st[0].fw[k], words.data(), n * sizeof(Word4<R>), cudaMemcpyHostToDevice));
             }
             for (int64_t p = 0; p < n; ++p) tmp[p] = R(1);
             GMPM_TRY(cudaMemcpy(st[0].c, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
-            GMPM_TRY(cudaMemset(st[0].alpha, 0, n * sizeof(R)));
-            GMPM_TRY(cudaMemset(st[0].psi, 0, n * sizeof(R)));
             std::vector<uint32_t> ids((size_t)n);
             for (int64_t p = 0; p < n; ++p)
                 ids[p] = (uint32_t)p | ((uint32_t)(init->material_ids ? init->material_ids[p] : 0) << 28);
@@ -595,10 +599,8 @@ struct Scene : SceneBase {
     template <typename F>
     void for_each_plane(int c, F&& f) {
         for (int a = 0; a < 3; ++a) f(st[c].x[a], sizeof(R));
-        for (int q = 0; q < 9; ++q) f(st[c].F[q], sizeof(R));
+        for (int k = 0; k < 3; ++k) f(st[c].fw[k], sizeof(Word4<R>));
         f(st[c].c, sizeof(R));
-        f(st[c].alpha, sizeof(R));
-        f(st[c].psi, sizeof(R));
         f(st[c].m, sizeof(R));
         f(st[c].id, sizeof(uint32_t));
         for (int a = 0; a < 3; ++a) f(aux.v[a], sizeof(R));
@@ -626,7 +628,7 @@ struct Scene : SceneBase {
         FILE* f = std::fopen(path, "wb");
         if (!f) return GMPM_IO_ERROR;
         bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 && std::fwrite(&desc, sizeof(desc), 1, f) == 1;
-        std::vector<unsigned char> buf((size_t)n * sizeof(double));
+        std::vector<unsigned char> buf((size_t)n * sizeof(Word4<double>));
         for_each_plane(cur, [&](const void* p, size_t esz) {
             if (!ok) return;
             ok = cudaMemcpy(buf.data(), p, (size_t)n * esz, cudaMemcpyDeviceToHost) == cudaSuccess &&
@@ -638,7 +640,7 @@ struct Scene : SceneBase {
 
     // Overwrite the freshly created state with a snapshot's planes and clock.
     gmpm_status restore(FILE* f, const SnapshotHeader& h) {
-        std::vector<unsigned char> buf((size_t)n * sizeof(double));
+        std::vector<unsigned char> buf((size_t)n * sizeof(Word4<double>));
         bool ok = true;
         for_each_plane(cur, [&](void* p, size_t esz) {
             if (!ok) return;
@@ -1131,7 +1133,8 @@ gmpm_status gmpm_scene_load(gmpm_context* ctx, const char* path, gmpm_scene** ou
     if (h.real_bytes != rb) return GMPM_IO_ERROR;
     const long base = std::ftell(f);
     const int64_t n = h.n;
-    // positions (planes 0-2), mass (plane 15) and ids (plane 16) build the scene;
+    // positions (planes 0-2), mass (plane 16) and ids (plane 17, counted in
+    // real-sized planes: x 3, the three words 12, c 1, m 1) build the scene;
     // then every plane is restored over it
     std::vector<double> pos((size_t)n * 3), mass((size_t)n);
     std::vector<int32_t> mat((size_t)n);
@@ -1147,9 +1150,9 @@ gmpm_status gmpm_scene_load(gmpm_context* ctx, const char* path, gmpm_scene** ou
         };
         for (int a = 0; a < 3; ++a)
             if (!read_plane(a, pos, 3, a)) return GMPM_IO_ERROR;
-        if (!read_plane(15, mass, 1, 0)) return GMPM_IO_ERROR;
+        if (!read_plane(16, mass, 1, 0)) return GMPM_IO_ERROR;
         std::vector<uint32_t> ids((size_t)n);
-        if (std::fseek(f, base + (long)(16 * n * (int64_t)rb), SEEK_SET) != 0 ||
+        if (std::fseek(f, base + (long)(17 * n * (int64_t)rb), SEEK_SET) != 0 ||
             std::fread(ids.data(), 4, (size_t)n, f) != (size_t)n)
             return GMPM_IO_ERROR;
         for (int64_t p = 0; p < n; ++p) mat[(size_t)p] = (int32_t)(ids[(size_t)p] >> 28);

@@ -36,7 +36,7 @@ namespace gmpm {
 // kPageRing (units k .. k+2 span at most 9 pages, units k and k+1 at most 6).
 constexpr int kG2PUnit = 256;
 constexpr int kG2PMinBlocks = 2;  // resident CTAs per SM (FP32), bounded by registers
-constexpr int kPlanesR = 16;  // x0..2, F0..8, c, alpha, psi, m
+constexpr int kPlanesR = 5;   // x0..2, c, m (F, alpha and psi travel as three words)
 constexpr int kUnitPages = 3;
 constexpr int kWinRing = 8;
 constexpr int kPageRing = 16;
@@ -49,6 +49,7 @@ struct G2PShared {
     R win4[kWinRing][kWindowNodes][4];  // (v0, v1, v2, dc) per window node
     R wincn[kWinRing][kWindowNodes];    // c_new per window node
     R p[2][kPlanesR][kG2PUnit];          // staged particle inputs; 2 unit buffers
+    Word4<R> pw[2][3][kG2PUnit];         // staged F / alpha / psi words; 2 unit buffers
     uint32_t id[2][kG2PUnit];
     int32_t o[3][kG2PUnit];              // previous slot per unit slot; 3 meta buffers
     uint32_t key[3][kG2PUnit];
@@ -60,7 +61,16 @@ struct G2PShared {
     uint32_t wtab[kGridChannels * kWindowNodes];
 };
 
-enum : int { P_X = 0, P_F = 3, P_C = 12, P_ALPHA = 13, P_PSI = 14, P_M = 15 };
+enum : int { P_X = 0, P_C = 3, P_M = 4 };
+
+// One particle word: one 16-byte copy in FP32, two in FP64.
+template <typename R>
+__device__ __forceinline__ void cp_async_word(Word4<R>* dst, const Word4<R>* src) {
+    static_assert(sizeof(Word4<R>) % 16 == 0, "whole 16-byte copies");
+#pragma unroll
+    for (int h = 0; h < (int)(sizeof(Word4<R>) / 16); ++h)
+        cp_async<16>(reinterpret_cast<char*>(dst) + 16 * h, reinterpret_cast<const char*>(src) + 16 * h);
+}
 
 // quadratic B-spline weights and gradients on nodes base+0..2 along one axis,
 // xp relative to the base node (G2PKernal.cu:257-288)
@@ -172,10 +182,8 @@ __device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int 
 #pragma unroll
         for (int a = 0; a < 3; ++a) cp_async_elem(&S.p[buf][P_X + a][t], in.x[a] + o);
 #pragma unroll
-        for (int q = 0; q < 9; ++q) cp_async_elem(&S.p[buf][P_F + q][t], in.F[q] + o);
+        for (int k = 0; k < 3; ++k) cp_async_word(&S.pw[buf][k][t], in.fw[k] + o);
         cp_async_elem(&S.p[buf][P_C][t], in.c + o);
-        cp_async_elem(&S.p[buf][P_ALPHA][t], in.alpha + o);
-        cp_async_elem(&S.p[buf][P_PSI][t], in.psi + o);
         cp_async_elem(&S.p[buf][P_M][t], in.m + o);
         cp_async_elem(&S.id[buf][t], in.id + o);
     }
@@ -381,6 +389,8 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
             const uint32_t idw = S.id[buf][t];
             out.id[slot] = idw;
             // F <- (I + dt grad v) F  (G2PKernal.cu:372-404)
+            const Word4<R> w0 = S.pw[buf][0][t], w1 = S.pw[buf][1][t], w2 = S.pw[buf][2][t];
+            const R Fi[9] = {w0.v[0], w0.v[1], w0.v[2], w0.v[3], w1.v[0], w1.v[1], w1.v[2], w1.v[3], w2.v[0]};
             R Fo[9];
             {
                 R A[9];
@@ -393,14 +403,13 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
                 for (int r = 0; r < 3; ++r)
 #pragma unroll
                     for (int c = 0; c < 3; ++c)
-                        Fo[r + 3 * c] = A[r] * S.p[buf][P_F + 3 * c][t] + A[r + 3] * S.p[buf][P_F + 3 * c + 1][t] +
-                                        A[r + 6] * S.p[buf][P_F + 3 * c + 2][t];
+                        Fo[r + 3 * c] = A[r] * Fi[3 * c] + A[r + 3] * Fi[3 * c + 1] + A[r + 6] * Fi[3 * c + 2];
             }
             const int mat = (int)(idw >> 28);
             const MaterialDev<R>& M = sc->mat[mat];
             const R theta = M.theta;
             const R g_old = c_old * c_old * (R(1) - theta) + theta;
-            const R alpha_in = S.p[buf][P_ALPHA][t], psi_in = S.p[buf][P_PSI][t];
+            const R alpha_in = w2.v[1], psi_in = w2.v[2];
             StressOut<R> so;
             constitutive_update<R, R, kAnyModel>(M, V0, dx, Fo, g_old, alpha_in, c_new, psi_in, so);
             if (fallback && so.smin_over_smax < ratio) {
@@ -427,14 +436,12 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
 #pragma unroll
             for (int a = 0; a < 3; ++a) aux.q[a][slot] = qs * gc[a];
 #pragma unroll
-            for (int q = 0; q < 9; ++q) {
-                out.F[q][slot] = so.F[q];
-                finite = finite && isfinite(so.F[q]);
-            }
+            for (int q = 0; q < 9; ++q) finite = finite && isfinite(so.F[q]);
+            out.fw[0][slot] = Word4<R>{{so.F[0], so.F[1], so.F[2], so.F[3]}};
+            out.fw[1][slot] = Word4<R>{{so.F[4], so.F[5], so.F[6], so.F[7]}};
+            out.fw[2][slot] = Word4<R>{{so.F[8], so.alpha, so.psi, R(0)}};
 #pragma unroll
             for (int q = 0; q < 6; ++q) aux.sigma[q][slot] = so.sigma[q];
-            out.alpha[slot] = so.alpha;
-            out.psi[slot] = so.psi;
             aux.vol[slot] = so.vol;
             aux.FP[slot] = so.FP;
             if (!finite) flags |= GMPM_FLAG_NONFINITE;

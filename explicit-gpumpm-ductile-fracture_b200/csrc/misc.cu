@@ -18,22 +18,22 @@ __global__ void k_init_stress(const SceneDev<R>* __restrict__ sc, PState<R> st, 
     if (p >= n) return;
     R F[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) F[q] = st.F[q][p];
+    for (int q = 0; q < 9; ++q) F[q] = st.F(q, p);
     const int mat = (int)(st.id[p] >> 28);
     StressOut<R> so;
-    constitutive_update<R, R>(sc->mat[mat], sc->V0, sc->dx, F, R(1), st.alpha[p], st.c[p], st.psi[p], so);
+    constitutive_update<R, R>(sc->mat[mat], sc->V0, sc->dx, F, R(1), st.alpha(p), st.c[p], st.psi(p), so);
     if (!so.svd_ok) raise_flag(cnt, GMPM_FLAG_SVD_NOCONVERGE);
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
-        st.F[q][p] = so.F[q];
+        st.F(q, p) = so.F[q];
         aux.B[q][p] = R(0);
     }
 #pragma unroll
     for (int q = 0; q < 6; ++q) aux.sigma[q][p] = so.sigma[q];
 #pragma unroll
     for (int a = 0; a < 3; ++a) aux.q[a][p] = R(0);
-    st.alpha[p] = so.alpha;
-    st.psi[p] = so.psi;
+    st.alpha(p) = so.alpha;
+    st.psi(p) = so.psi;
     aux.vol[p] = so.vol;
     aux.FP[p] = so.FP;
 }
@@ -113,6 +113,7 @@ template cudaError_t launch_particle_diag<double>(const PState<double>&, const P
 
 struct FieldPlanes {
     const void* plane[9];
+    int step[9];  // elements between particles: 1 for a plane, 4 for a component of a four-wide word
     int comps;
     int is_id;
 };
@@ -120,18 +121,26 @@ struct FieldPlanes {
 template <typename R>
 __host__ FieldPlanes field_planes(const PState<R>& st, const PAux<R>& aux, int field) {
     FieldPlanes f{};
+    for (int q = 0; q < 9; ++q) f.step[q] = 1;
     auto set = [&](int nc, auto* const* planes) {
         f.comps = nc;
         for (int q = 0; q < nc; ++q) f.plane[q] = planes[q];
     };
+    auto word_component = [&](int slot, int q) {  // F(q) for q < 9; alpha and psi_max follow F8
+        f.plane[slot] = reinterpret_cast<const R*>(st.fw[q >> 2]) + (q & 3);
+        f.step[slot] = 4;
+    };
     switch (field) {
         case GMPM_FIELD_POSITION: set(3, st.x); break;
         case GMPM_FIELD_VELOCITY: set(3, aux.v); break;
-        case GMPM_FIELD_F: set(9, st.F); break;
+        case GMPM_FIELD_F:
+            f.comps = 9;
+            for (int q = 0; q < 9; ++q) word_component(q, q);
+            break;
         case GMPM_FIELD_B: set(9, aux.B); break;
         case GMPM_FIELD_DAMAGE: f.comps = 1; f.plane[0] = st.c; break;
-        case GMPM_FIELD_ALPHA: f.comps = 1; f.plane[0] = st.alpha; break;
-        case GMPM_FIELD_PSI_MAX: f.comps = 1; f.plane[0] = st.psi; break;
+        case GMPM_FIELD_ALPHA: f.comps = 1; word_component(0, 9); break;
+        case GMPM_FIELD_PSI_MAX: f.comps = 1; word_component(0, 10); break;
         case GMPM_FIELD_STRESS: set(6, aux.sigma); break;
         case GMPM_FIELD_VOLUME: f.comps = 1; f.plane[0] = aux.vol; break;
         case GMPM_FIELD_FP: f.comps = 1; f.plane[0] = aux.FP; break;
@@ -155,7 +164,7 @@ __global__ void k_pack_field(FieldPlanes f, const uint32_t* __restrict__ ids, in
         if (f.is_id)
             v = (double)(reinterpret_cast<const uint32_t*>(f.plane[q])[p] & 0x0fffffffu);
         else
-            v = (double)reinterpret_cast<const R*>(f.plane[q])[p];
+            v = (double)reinterpret_cast<const R*>(f.plane[q])[p * f.step[q]];
         const int64_t e = dst * f.comps + q;
         if (dtype == GMPM_DTYPE_F64)
             reinterpret_cast<double*>(out)[e] = v;

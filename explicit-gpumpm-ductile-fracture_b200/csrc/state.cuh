@@ -13,17 +13,29 @@
 
 namespace gmpm {
 
+// Four values of one particle in one aligned word (16 bytes in FP32), so that
+// a gather through perm moves them with one wide copy.
+template <typename R>
+struct __align__(16) Word4 {
+    R v[4];
+};
+
 // Fields that G2P reads through perm and rewrites in sorted order: double-buffered.
+// Only G2P reads F and the plastic state, so those travel as three words per
+// particle: fw[0] = (F0, F1, F2, F3), fw[1] = (F4, F5, F6, F7),
+// fw[2] = (F8, alpha, psi_max, 0), with F column-major (element (r, c) at
+// r + 3c).  The other kernels read x, c and m, which stay one plane each.
 template <typename R>
 struct PState {
     R* x[3];
-    R* F[9];
+    Word4<R>* fw[3];
     R* c;
-    R* alpha;
-    R* psi;
     R* m;
     uint32_t* id;    // (material << 28) | original index
     int64_t stride;  // elements per plane (>= n + kPlanePad), shared by every particle plane
+    __host__ __device__ R& F(int q, int64_t p) const { return fw[q >> 2][p].v[q & 3]; }
+    __host__ __device__ R& alpha(int64_t p) const { return fw[2][p].v[1]; }
+    __host__ __device__ R& psi(int64_t p) const { return fw[2][p].v[2]; }
 };
 
 // Padding of every particle plane beyond n, so a window of kPlanePad previous
