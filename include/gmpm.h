@@ -429,7 +429,9 @@ gmpm_status gmpm_sample_sdf(const char* path, const uint32_t center[3], const ui
  * plane of the state in the internal order (the reference's Attribs_Back_Host, Particles.cpp:33-52,
  * and its declared but undefined writePartio, Simulator.h:35, as a restartable file).  Binning and grid
  * are rebuilt by the next substep, so a loaded scene continues bitwise like the original in
- * deterministic mode.  The file is tied to the library's struct layouts (native byte order). */
+ * deterministic mode.  The file is tied to the library's struct layouts (native byte order) and carries
+ * a format version: a file written by a build with another particle layout is refused with
+ * GMPM_IO_ERROR. */
 gmpm_status gmpm_scene_save(gmpm_scene* scene, const char* path);
 gmpm_status gmpm_scene_load(gmpm_context* ctx, const char* path, gmpm_scene** out);
 
