@@ -27,7 +27,9 @@ namespace gmpm {
 // A CTA walks its units with a three-deep software pipeline of asynchronous
 // copies:
 //   unit k+2: perm, sorted keys, and its pages' adjacency rows and keys  (meta)
-//   unit k+1: the particles' 17 input words (through perm) and the 6x6x6
+//   unit k+1: the particles' inputs through perm (x, c, m, id one value per
+//             copy; F, alpha and psi_max as three four-wide words, one
+//             16-byte copy each in FP32) and the 6x6x6
 //             node window of each page not staged yet                    (data)
 //   unit k  : computed from shared memory
 // so global latency is hidden behind the previous unit's arithmetic.  Pages
