@@ -163,7 +163,8 @@ void fill_scene_dev(const gmpm_scene_desc& d, int key_bits, SceneDev<R>& s) {
         o.fracture_energy = (R)in.fracture_energy;
         o.softening_onset = (R)in.softening_onset;
         o.residual_fracture = (R)in.residual_fracture;
-        o.theta = (R)in.theta;
+        o.theta = (R)(float)in.theta;
+        o.one_minus_theta = (R)(1.0f - (float)in.theta);
         o.length_scale = (R)in.length_scale;
         o.mobility = (R)in.mobility;
     }

@@ -43,6 +43,7 @@ struct MaterialDev {
     Real alpha_cap, dlambda_cap, strain_cap, psi_cap;
     Real fracture_energy, softening_onset, residual_fracture;
     Real theta, length_scale, mobility;
+    Real one_minus_theta;   // (1 - theta) rounded to float: theta is a float in the reference (:334)
 };
 
 // Velocity conditions: axis-aligned slabs and moving spheres.  Kept as one

@@ -140,11 +140,11 @@ __device__ __forceinline__ void von_mises_from_svd(const MaterialDev<MR>& m, R V
     else
         Gc = R(m.fracture_energy) *
              (((R(1) - R(m.residual_fracture)) * exp_r(R(m.softening_onset) - p)) + R(m.residual_fracture));
-    const R theta = R(m.theta);
-    o.FP = R(4) * R(m.length_scale) * (R(1) - theta) * psi * (R(1) / Gc) + R(1);
+    const R theta = R(m.theta), one_minus_theta = R(m.one_minus_theta);
+    o.FP = R(4) * R(m.length_scale) * one_minus_theta * psi * (R(1) / Gc) + R(1);
     const R tvol = (kappa * R(0.5)) * (J * J - R(1));
     const R third = (R(1) / R(3)) * bbs;
-    const R gn = c * c * (R(1) - theta) + theta;
+    const R gn = c * c * one_minus_theta + theta;
     R Ph[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {

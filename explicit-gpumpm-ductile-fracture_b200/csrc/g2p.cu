@@ -409,8 +409,7 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
             }
             const int mat = (int)(idw >> 28);
             const MaterialDev<R>& M = sc->mat[mat];
-            const R theta = M.theta;
-            const R g_old = c_old * c_old * (R(1) - theta) + theta;
+            const R g_old = c_old * c_old * M.one_minus_theta + M.theta;
             const R alpha_in = w2.v[1], psi_in = w2.v[2];
             StressOut<R> so;
             constitutive_update<R, R, kAnyModel>(M, V0, dx, Fo, g_old, alpha_in, c_new, psi_in, so);

@@ -614,14 +614,17 @@ void von_mises(const MatConsts& mc, double V0, const double* Fin, double g, doub
     else
         Gc = m->fracture_energy * (((1.0 - m->residual_fracture) * std::exp(m->softening_onset - p)) +
                                    m->residual_fracture);
-    const double theta = m->theta;
+    // theta is a float in the reference (`float theta = 0.0001f`, :334), so
+    // (1 - theta) is a single-precision difference promoted to double.
+    const double theta = (double)(float)m->theta;
+    const double one_minus_theta = (double)(1.0f - (float)m->theta);
     const double L0 = m->length_scale;
-    const double FP = 4 * L0 * (1 - theta) * psi * (1.0 / Gc) + 1.0;
+    const double FP = 4 * L0 * one_minus_theta * psi * (1.0 / Gc) + 1.0;
     const double tvol = (kappa * 0.5) * (J * J - 1.0);
     const double third = (1.0 / 3.0) * bbs;
     double tdev[3];
     for (int k = 0; k < 3; ++k) tdev[k] = mu * (bb[k] - third);
-    const double gn = c * c * (1 - theta) + theta;
+    const double gn = c * c * one_minus_theta + theta;
     double Ph[3];
     for (int k = 0; k < 3; ++k) Ph[k] = (J < 1.0) ? gn * tdev[k] + tvol : gn * (tdev[k] + tvol);
     double P[9];
@@ -817,16 +820,20 @@ void permute(std::vector<T>& a, const std::vector<int32_t>& perm, int comps) {
 
 // Key of a particle's stencil base node ⌊x/dx + 0.5⌋ - 1 (cal_cellId,
 // Particle_kernal.cu:158-165), with the bounds check the reference lacks.
-void base_node(const orc_scene& s, const double* xp, int b[3], uint32_t* flags) {
+void base_node_of(double inv_dx, const int32_t* res, const double* xp, int b[3], uint32_t* flags) {
     for (int a = 0; a < 3; ++a) {
-        int i = (int)(xp[a] * s.inv_dx + 0.5) - 1;
-        const int hi = s.desc.grid_res[a] - 3;
-        if (!(xp[a] * s.inv_dx + 0.5 >= 1.0) || i > hi) {
+        int i = (int)(xp[a] * inv_dx + 0.5) - 1;
+        const int hi = res[a] - 3;
+        if (!(xp[a] * inv_dx + 0.5 >= 1.0) || i > hi) {
             *flags |= GMPM_FLAG_OUT_OF_DOMAIN;
             i = std::min(std::max(i, 0), hi);
         }
         b[a] = i;
     }
+}
+
+void base_node(const orc_scene& s, const double* xp, int b[3], uint32_t* flags) {
+    base_node_of(s.inv_dx, s.desc.grid_res, xp, b, flags);
 }
 
 uint32_t rebin(orc_scene& s) {
@@ -1137,12 +1144,59 @@ void pcg_phase_field(orc_scene& s) {
 // explicit phase-field update, velocity conditions (PullGrid_kernal,
 // TimeIntegrator.cu:169-261, generalised) and the sticky walls of
 // collideWithGround (TimeIntegrator.cu:117-165).
+// Node velocity of undateGrid_kernal (TimeIntegrator.cu:63-111): v = p/m, then
+// gravity (the reference's hard-coded -10 dt on y; a parameter here), then the
+// force term f dt/m where it is finite.
+void node_velocity(const gmpm_scene_desc& d, double mass, const double* p, const double* f, double vel[3]) {
+    const double dt = d.dt;
+    const double im = 1.0 / mass;
+    for (int a = 0; a < 3; ++a) vel[a] = p[a] * im;
+    for (int a = 0; a < 3; ++a) vel[a] += d.gravity[a] * dt;
+    const double dtm = dt * im;
+    for (int a = 0; a < 3; ++a) {
+        const double test = f[a] * dtm;
+        if (std::isfinite(test)) vel[a] += test;
+    }
+}
+
+// Velocity conditions at grid node idx, in the reference's order: slabs (the
+// configs' end pulls), moving spheres (PullGrid_kernal, TimeIntegrator.cu:
+// 169-214, later spheres winning), then the sticky walls within wall_layers
+// nodes of each face, x low/high, y, z, each zeroing all three components
+// (collideWithGround, :117-165).
+void velocity_conditions(const gmpm_scene_desc& d, double t_now, const int idx[3], double vel[3]) {
+    const double pos[3] = {idx[0] * d.dx, idx[1] * d.dx, idx[2] * d.dx};
+    for (int sb = 0; sb < d.n_slab_bcs; ++sb) {
+        const gmpm_slab_bc& sl = d.slabs[sb];
+        if (pos[sl.axis] >= sl.lo && pos[sl.axis] <= sl.hi)
+            for (int a = 0; a < 3; ++a) vel[a] = sl.velocity[a];
+    }
+    for (int sp = 0; sp < d.n_sphere_bcs; ++sp) {
+        const gmpm_sphere_bc& b = d.spheres[sp];
+        double d2 = 0;
+        for (int a = 0; a < 3; ++a) {
+            const double dd = pos[a] - (b.center[a] + b.velocity[a] * t_now);
+            d2 += dd * dd;
+        }
+        if (d2 < b.radius * b.radius)
+            for (int a = 0; a < 3; ++a) vel[a] = b.velocity[a];
+    }
+    if (d.wall_bc) {
+        const int L = d.wall_layers;
+        for (int a = 0; a < 3; ++a) {
+            const int N = d.grid_res[a];
+            if (idx[a] <= L && vel[a] < 0.0) vel[0] = vel[1] = vel[2] = 0.0;
+            if (idx[a] > N - L && vel[a] > 0.0) vel[0] = vel[1] = vel[2] = 0.0;
+        }
+    }
+}
+
 void grid_update(orc_scene& s) {
     const int64_t ng = (int64_t)s.grid_keys.size();
     s.gv.assign(ng * 64 * 3, 0.0);
     s.gdc.assign(ng * 64, 0.0);
     s.gcn.assign(ng * 64, 0.0);
-    const double dt = s.desc.dt, dx = s.dx, t_now = s.time;
+    const double dt = s.desc.dt, t_now = s.time;
     const double Mob = s.desc.materials[0].mobility;
     const bool pf = s.desc.phase_field == GMPM_PHASE_FIELD_EXPLICIT;
     const bool pcg = s.desc.phase_field == GMPM_PHASE_FIELD_IMPLICIT;
@@ -1180,14 +1234,8 @@ void grid_update(orc_scene& s) {
             gp1 += ch[CH_P1] + dt * ch[CH_F1];
             gp2 += ch[CH_P2] + dt * ch[CH_F2];
             const double cgrid = ch[CH_CW] / ch[CH_W];
-            const double im = 1.0 / mass;
-            double vel[3] = {ch[CH_P0] * im, ch[CH_P1] * im, ch[CH_P2] * im};
-            for (int a = 0; a < 3; ++a) vel[a] += s.desc.gravity[a] * dt;
-            const double dtm = dt * im;
-            for (int a = 0; a < 3; ++a) {
-                const double test = ch[CH_F0 + a] * dtm;
-                if (std::isfinite(test)) vel[a] += test;
-            }
+            double vel[3];
+            node_velocity(s.desc, mass, &ch[CH_P0], &ch[CH_F0], vel);
             // explicit phase field (see file header)
             double cnew = cgrid;
             if (pf) {
@@ -1203,33 +1251,8 @@ void grid_update(orc_scene& s) {
                 s.pcg_cg[gi] = cgrid;
                 s.pcg_tag[gi] = 1;
             }
-            // velocity conditions
-            const int I = 4 * gx + ci, J = 4 * gy + cj, K = 4 * gz + ck;
-            const double pos[3] = {I * dx, J * dx, K * dx};
-            for (int sb = 0; sb < s.desc.n_slab_bcs; ++sb) {
-                const gmpm_slab_bc& sl = s.desc.slabs[sb];
-                if (pos[sl.axis] >= sl.lo && pos[sl.axis] <= sl.hi)
-                    for (int a = 0; a < 3; ++a) vel[a] = sl.velocity[a];
-            }
-            for (int sp = 0; sp < s.desc.n_sphere_bcs; ++sp) {
-                const gmpm_sphere_bc& b = s.desc.spheres[sp];
-                double d2 = 0;
-                for (int a = 0; a < 3; ++a) {
-                    const double dd = pos[a] - (b.center[a] + b.velocity[a] * t_now);
-                    d2 += dd * dd;
-                }
-                if (d2 < b.radius * b.radius)
-                    for (int a = 0; a < 3; ++a) vel[a] = b.velocity[a];
-            }
-            if (s.desc.wall_bc) {
-                const int L = s.desc.wall_layers;
-                const int idx[3] = {I, J, K};
-                for (int a = 0; a < 3; ++a) {
-                    const int N = s.desc.grid_res[a];
-                    if (idx[a] <= L && vel[a] < 0.0) vel[0] = vel[1] = vel[2] = 0.0;
-                    if (idx[a] > N - L && vel[a] > 0.0) vel[0] = vel[1] = vel[2] = 0.0;
-                }
-            }
+            const int node_idx[3] = {4 * gx + ci, 4 * gy + cj, 4 * gz + ck};
+            velocity_conditions(s.desc, t_now, node_idx, vel);
             for (int a = 0; a < 3; ++a) s.gv[gi * 3 + a] = vel[a];
             s.gdc[gi] = cnew - cgrid;
             s.gcn[gi] = cnew;
@@ -1378,6 +1401,23 @@ void orc_constitutive(const gmpm_material* mat, double V0, double dx, const doub
     out[12] = o.FP;
     for (int q = 0; q < 9; ++q) out[13 + q] = o.contrib[q];
     out[22] = o.vol;
+}
+
+int orc_base_node(double inv_dx, const int32_t res[3], const double x[3], int32_t out[3]) {
+    uint32_t flags = 0;
+    int b[3];
+    base_node_of(inv_dx, res, x, b, &flags);
+    for (int a = 0; a < 3; ++a) out[a] = b[a];
+    return (int)flags;
+}
+
+void orc_grid_node(const gmpm_scene_desc* desc, double t, const int32_t node[3], const double ch[9], double out[4]) {
+    double vel[3];
+    node_velocity(*desc, ch[0], &ch[1], &ch[4], vel);
+    const int idx[3] = {node[0], node[1], node[2]};
+    velocity_conditions(*desc, t, idx, vel);
+    for (int a = 0; a < 3; ++a) out[a] = vel[a];
+    out[3] = ch[7] / ch[8];
 }
 
 void orc_set_threads(int n) {

@@ -9,10 +9,12 @@
  *
  * Pinning: the SPGrid masks and Linear_Offset, the material constants and the
  * 3x3 SVD are checked against the reference's own code compiled here
- * (oracle/_ref/ref_kat, fixtures in tests/golden/).  The remaining kernels
- * (applyVonMises, P2G_APIC, undateGrid_kernal, collideWithGround, G2P_APIC,
- * binning) are __global__/__device__-only in the reference and are checked by
- * invariants and hand-derived identities.
+ * (oracle/_ref/ref_kat), and so are the per-thread kernels applyVonMises,
+ * computePhase_field_vol, undateGrid_kernal, collideWithGround, PullGrid_kernal,
+ * cal_cellId and calcIndex, run serially on the host (oracle/_ref/ref_kernels);
+ * fixtures in tests/golden/.  P2G_APIC, G2P_APIC and the binning use shared
+ * memory, warp reductions and atomics; they are checked by invariants and
+ * hand-derived identities.
  */
 #ifndef GMPM_ORACLE_H
 #define GMPM_ORACLE_H
@@ -47,6 +49,19 @@ void orc_von_mises(const gmpm_material* mat, double V0, const double* io, double
  * von Mises, fixed-corotated or Neo-Hookean with fracture); dx sets the
  * Neo-Hookean phase-field length L0 = dx/2.  Same io / out layout. */
 void orc_constitutive(const gmpm_material* mat, double V0, double dx, const double* io, double* out);
+
+/* Stencil base node floor(x/dx + 0.5) - 1 of one particle (cal_cellId,
+ * Particle_kernal.cu:158-165, and calcIndex, TimeIntegrator.cu:53-61), clamped
+ * into [0, res - 3] per axis; returns GMPM_FLAG_OUT_OF_DOMAIN if it was not
+ * inside. */
+int orc_base_node(double inv_dx, const int32_t res[3], const double x[3], int32_t out[3]);
+
+/* One grid node of the grid update (undateGrid_kernal, TimeIntegrator.cu:63-111)
+ * followed by the scene's velocity conditions (slabs, spheres as in
+ * PullGrid_kernal :169-214, sticky walls as in collideWithGround :117-165) at
+ * simulated time t.  ch: mass, momentum xyz, force xyz, sum w c, sum w.
+ * out: velocity xyz, c = sum w c / sum w (FP64 division). */
+void orc_grid_node(const gmpm_scene_desc* desc, double t, const int32_t node[3], const double ch[9], double out[4]);
 
 typedef struct orc_scene orc_scene;
 

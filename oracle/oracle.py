@@ -45,6 +45,9 @@ def lib(desc_type=None, diag_type=None, material_type=None) -> C.CDLL:
         L.orc_lame.argtypes = [C.c_double, C.c_double, dp, dp, dp]
         L.orc_von_mises.argtypes = [vp, C.c_double, dp, dp]
         L.orc_constitutive.argtypes = [vp, C.c_double, C.c_double, dp, dp]
+        L.orc_base_node.restype = C.c_int
+        L.orc_base_node.argtypes = [C.c_double, ip, dp, ip]
+        L.orc_grid_node.argtypes = [vp, C.c_double, ip, dp, dp]
         L.orc_scene_create.restype = vp
         L.orc_scene_create.argtypes = [vp, C.c_int64, dp, dp, dp, ip]
         L.orc_scene_destroy.argtypes = [vp]

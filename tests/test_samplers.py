@@ -6,6 +6,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -13,7 +14,10 @@ import pytest
 
 GOLDEN = Path(__file__).parent / "golden"
 GOLD = json.loads((GOLDEN / "reference_kats.json").read_text())
-TUBE = Path("/root/reference/Assets/sample/tube_10.obj")
+# the reference's one shipped OBJ asset, where the reference project is present
+# (its root in the environment variable GMPM_REFERENCE_DIR)
+_REF = os.environ.get("GMPM_REFERENCE_DIR", "")
+TUBE = Path(_REF) / "Assets" / "sample" / "tube_10.obj" if _REF else None
 
 
 def _check(pos: np.ndarray, rec: dict):
@@ -33,7 +37,7 @@ def test_obj_records_match_reference(pkg):
     assert len(pos) == 112
 
 
-@pytest.mark.skipif(not TUBE.exists(), reason="the reference's tube_10.obj asset is not present")
+@pytest.mark.skipif(TUBE is None or not TUBE.exists(), reason="the reference's tube_10.obj asset is not present")
 def test_tube_10_obj_matches_reference(pkg):
     _check(pkg.gmpm.sample_obj(TUBE), GOLD["sample_tube_10_obj"])
 
