@@ -289,19 +289,18 @@ static unsigned bin_grid(int64_t n) {
 
 cudaError_t launch_bin_hist(int64_t n, const uint32_t* keys, const int32_t* page_rank, int32_t* cell_count, int nb_cap,
                             cudaStream_t s) {
-    k_bin_hist<<<bin_grid(n), kBinThreads, 0, s>>>(n, keys, page_rank, cell_count, nb_cap);
-    return cudaGetLastError();
+    return launch_kernel(k_bin_hist, dim3(bin_grid(n)), dim3(kBinThreads), 0, s, n, keys, page_rank, cell_count,
+                         nb_cap);
 }
 
 cudaError_t launch_bin_scatter(int64_t n, const uint32_t* keys, const int32_t* page_rank, const int32_t* cell_start,
                                int32_t* fill, int32_t* perm, uint32_t* keys_sorted, int nb_cap, cudaStream_t s) {
-    k_bin_scatter<<<bin_grid(n), kBinThreads, 0, s>>>(n, keys, page_rank, cell_start, fill, perm, keys_sorted, nb_cap);
-    return cudaGetLastError();
+    return launch_kernel(k_bin_scatter, dim3(bin_grid(n)), dim3(kBinThreads), 0, s, n, keys, page_rank, cell_start,
+                         fill, perm, keys_sorted, nb_cap);
 }
 
 cudaError_t launch_bin_canon(BinDev bin, Counters* cnt, int num_sms, cudaStream_t s) {
-    k_bin_canon<<<num_sms * 8, 32 * kCanonWarps, 0, s>>>(bin, cnt);
-    return cudaGetLastError();
+    return launch_kernel(k_bin_canon, dim3(num_sms * 8), dim3(32 * kCanonWarps), 0, s, bin, cnt);
 }
 
 template <typename R>

@@ -13,11 +13,15 @@
 // GPU (different streams, or host threads without ordering) race on it and
 // must be serialised by the caller.  Its contents persist between calls, so
 // everything that must start at zero is cleared on the call's stream first.
+// The work is enqueued on the caller's stream, which must belong to the
+// current device (the array resolved is the current device's).
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
 
 #include "kernels.h"
+#include "launch.cuh"
 #include "scan.cuh"
 
 namespace gmpm {
@@ -106,7 +110,8 @@ cudaError_t scratch_for_current_device(unsigned char** out) {
 }  // namespace gmpm
 
 extern "C" gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_t n, double dx, int res_x, int res_y,
-                                                  int res_z, int32_t* perm, uint32_t* keys_sorted, void* stream) {
+                                                  int res_z, int32_t* perm, uint32_t* keys_sorted, uint32_t* flags,
+                                                  void* stream) {
     using namespace gmpm;
     if (!positions || !perm || !keys_sorted || n <= 0 || !(dx > 0)) return GMPM_INVALID_ARG;
     if (n > kNoAllocMaxParticles) return GMPM_INVALID_ARG;
@@ -114,16 +119,17 @@ extern "C" gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_
     for (int a = 0; a < 3; ++a)
         if (res[a] < 8 || res[a] > kNoAllocMaxRes) return GMPM_INVALID_ARG;
     unsigned char* base = nullptr;
-    if (scratch_for_current_device(&base) != cudaSuccess) {
-        cudaGetLastError();
-        return GMPM_CUDA_ERROR;
-    }
+    if (scratch_for_current_device(&base) != cudaSuccess) return GMPM_CUDA_ERROR;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     Counters* cnt = reinterpret_cast<Counters*>(base + kOffCounters);
+    // n particles occupy at most n pages, so page ranks stay below min(n, key space):
+    // only that many pages' cells are cleared and scanned
+    const int32_t nb_cap = (int32_t)std::min<int64_t>(n, (int64_t)kNoAllocKeySpace);
+    const int64_t ncell = (int64_t)nb_cap * 64;
     BinDev bin{};
     bin.n = n;
     bin.key_space = kNoAllocKeySpace;
-    bin.nb_cap = (int32_t)kNoAllocKeySpace;
+    bin.nb_cap = nb_cap;
     bin.ng_cap = 0;
     bin.keys = reinterpret_cast<uint32_t*>(base + kOffKeys);
     bin.keys_sorted = keys_sorted;
@@ -134,26 +140,34 @@ extern "C" gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_
     bin.cell_count = reinterpret_cast<int32_t*>(base + kOffCellCount);
     bin.cell_start = reinterpret_cast<int32_t*>(base + kOffCellStart);
     ScanScratch scan{reinterpret_cast<int32_t*>(base + kOffScanTiles), (int64_t)kScanTilesElems};
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 
     // state left by the previous call: clear what must start at zero
-    cudaMemsetAsync(cnt, 0, sizeof(Counters), s);
-    cudaMemsetAsync(bin.page_flag, 0, kNoAllocKeySpace, s);
-    cudaMemsetAsync(bin.cell_count, 0, kNoAllocCells * sizeof(int32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(Counters), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bin.page_flag, 0, kNoAllocKeySpace, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), s);
     const int T = 256;
     const unsigned gn = (unsigned)((n + T - 1) / T);
     const unsigned gk = (kNoAllocKeySpace + T - 1) / T;
-    k_noalloc_keys<<<gn, T, 0, s>>>(n, positions, 1.0 / dx, res_x, res_y, res_z, bin.keys, bin.page_flag, cnt);
-    scan_exclusive<uint8_t>(bin.page_flag, bin.page_rank, (int64_t)kNoAllocKeySpace, &cnt->n_blocks, scan, s);
-    k_compact_keys<<<gk, T, 0, s>>>(kNoAllocKeySpace, bin.page_flag, bin.page_rank, bin.block_keys, bin.nb_cap, cnt);
-    launch_bin_hist(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap, s);
-    scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, kNoAllocCells, bin.cell_start + kNoAllocCells, scan, s);
-    cudaMemsetAsync(bin.cell_count, 0, kNoAllocCells * sizeof(int32_t), s);
-    launch_bin_scatter(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, perm, keys_sorted, bin.nb_cap, s);
-    int sms = 148;
-    int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    launch_bin_canon(bin, cnt, sms, s);
-    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = launch_kernel(k_noalloc_keys, dim3(gn), dim3(T), 0, s, n, positions, 1.0 / dx, res_x, res_y, res_z,
+                          bin.keys, bin.page_flag, cnt);
+    if (e == cudaSuccess)
+        e = scan_exclusive<uint8_t>(bin.page_flag, bin.page_rank, (int64_t)kNoAllocKeySpace, &cnt->n_blocks, scan, s);
+    if (e == cudaSuccess)
+        e = launch_kernel(k_compact_keys, dim3(gk), dim3(T), 0, s, kNoAllocKeySpace, (const uint8_t*)bin.page_flag,
+                          (const int32_t*)bin.page_rank, bin.block_keys, (int)bin.nb_cap, cnt);
+    if (e == cudaSuccess) e = launch_bin_hist(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap, s);
+    if (e == cudaSuccess) e = scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, ncell, bin.cell_start + ncell, scan, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), s);
+    if (e == cudaSuccess)
+        e = launch_bin_scatter(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, perm, keys_sorted,
+                               bin.nb_cap, s);
+    if (e == cudaSuccess) e = launch_bin_canon(bin, cnt, sms, s);
+    if (e == cudaSuccess && flags)
+        e = cudaMemcpyAsync(flags, &cnt->flags, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? GMPM_OOM : GMPM_CUDA_ERROR;
     return GMPM_OK;
 }

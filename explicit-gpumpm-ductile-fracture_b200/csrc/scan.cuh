@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "launch.cuh"
+
 namespace gmpm {
 
 constexpr int kScanThreads = 256;
@@ -110,14 +112,19 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const TIn* __restri
     }
 }
 
-// out[i] = sum_{j<i} in[j] for i < n; *total = sum of all.
+// out[i] = sum_{j<i} in[j] for i < n; *total = sum of all.  Returns the
+// status of its own launches.
 template <typename TIn>
-inline void scan_exclusive(const TIn* in, int32_t* out, int64_t n, int32_t* total, ScanScratch s,
-                           cudaStream_t stream) {
+inline cudaError_t scan_exclusive(const TIn* in, int32_t* out, int64_t n, int32_t* total, ScanScratch s,
+                                  cudaStream_t stream) {
     const int64_t ntiles = (n + kScanTile - 1) / kScanTile;
-    k_scan_reduce<TIn><<<(unsigned)ntiles, kScanThreads, 0, stream>>>(in, n, s.tile_sums);
-    k_scan_tiles<<<1, kScanThreads, 0, stream>>>(s.tile_sums, ntiles, total);
-    k_scan_apply<TIn><<<(unsigned)ntiles, kScanThreads, 0, stream>>>(in, n, s.tile_sums, out);
+    cudaError_t e = launch_kernel(k_scan_reduce<TIn>, dim3((unsigned)ntiles), dim3(kScanThreads), 0, stream, in, n,
+                                  s.tile_sums);
+    if (e == cudaSuccess) e = launch_kernel(k_scan_tiles, dim3(1), dim3(kScanThreads), 0, stream, s.tile_sums, ntiles, total);
+    if (e == cudaSuccess)
+        e = launch_kernel(k_scan_apply<TIn>, dim3((unsigned)ntiles), dim3(kScanThreads), 0, stream, in, n,
+                          (const int32_t*)s.tile_sums, out);
+    return e;
 }
 
 inline int64_t scan_scratch_elems(int64_t max_n) { return (max_n + kScanTile - 1) / kScanTile + 1; }

@@ -170,7 +170,7 @@ SIGNATURES = {
     "gmpm_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Diag)]),
     "gmpm_status_string": (C.c_char_p, [C.c_int]),
     "gmpm_bin_positions_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_int, C.c_int, C.c_int,
-                                             C.c_void_p, C.c_void_p, C.c_void_p]),
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "gmpm_generate_particles": (C.c_int, [C.POINTER(Geometry), C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                           C.POINTER(C.c_int32), C.c_int64]),
     "gmpm_sample_obj": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int64]),

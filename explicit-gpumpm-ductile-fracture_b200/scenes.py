@@ -120,7 +120,7 @@ def notched_bar_batch(n_scenes: int = 64, seed: int = 0, lo: int = 10_000, hi: i
 
 
 def _plate_scene(name: str, cells_xy: int, dx: float, ppc: int, margin: int, gap: int, res_y: int, seed: int,
-                 precision: int, substeps: int) -> SceneSpec:
+                 precision: int, substeps: int, sphere_gap: float = 2.0) -> SceneSpec:
     n_plates = 4
     thick = 16
     res_xz = cells_xy + 2 * margin
@@ -144,7 +144,7 @@ def _plate_scene(name: str, cells_xy: int, dx: float, ppc: int, margin: int, gap
     d.n_sphere_bcs = 1
     sp = d.spheres[0]
     sp.center[0] = sp.center[2] = res_xz * dx / 2
-    sp.center[1] = top + r + 2 * dx
+    sp.center[1] = top + r + sphere_gap * dx
     sp.radius = r
     sp.velocity[1] = -5.0
     d.precision = precision
@@ -164,10 +164,40 @@ def plates_8m(seed: int = 0, precision: int = G.PRECISION_FP32, substeps: int = 
 
 
 def plates_small(cells_xy: int = 32, seed: int = 0, precision: int = G.PRECISION_FP32,
-                 substeps: int = 50) -> SceneSpec:
-    """Scaled-down plate-impact scene with the same parameters (test size)."""
+                 substeps: int = 50, sphere_gap: float = 2.0) -> SceneSpec:
+    """Scaled-down plate-impact scene with the same parameters (test size).
+    sphere_gap: height of the sphere's lowest point above the top plate, in
+    cells (0.5 puts the top layer of nodes with mass inside the sphere at once)."""
     dx = 1.0 / 128
-    return _plate_scene(f"plates_{cells_xy}", cells_xy, dx, 8, 8, 4, 96, seed, precision, substeps)
+    return _plate_scene(f"plates_{cells_xy}", cells_xy, dx, 8, 8, 4, 96, seed, precision, substeps, sphere_gap)
+
+
+def wall_slide(corner: str = "low", n_side: int = 8, ppc: int = 8, seed: int = 11, precision: int = G.PRECISION_FP32,
+               dx: float = 1.0 / 64, res: int = 48, speed: float = 2.0) -> SceneSpec:
+    """A box moving diagonally into a corner of the domain with the sticky
+    walls on (collideWithGround, TimeIntegrator.cu:117-165).  "low": the box's
+    lowest cells start at node 5 on every axis and it moves towards -x, -y, -z;
+    "high": its highest cells end at node res - 4 and it moves towards +x, +y,
+    +z.  Either way the stencils reach the wall layers (nodes i <= 4 and
+    i > res - 4) at once.  No gravity; elastic material."""
+    lo = 5 if corner == "low" else res - 4 - n_side
+    origin = (lo * dx,) * 3
+    geom = G.Geometry(kind=2, cells=(n_side, n_side, n_side), ppc=ppc, n_plates=1, gap_cells=0, notch_width=0,
+                      notch_depth=0, dx=dx, origin=origin, seed=seed)
+    pos, mat = G.generate_particles(geom)
+    d = G.reference_defaults(dx, (res, res, res))
+    d.dt = 1e-4
+    d.gravity[0] = d.gravity[1] = d.gravity[2] = 0.0
+    d.wall_bc = 1
+    d.wall_layers = 4
+    d.particle_volume = dx ** 3 / ppc
+    config_material(d.materials[0], dx)
+    d.materials[0].yield_stress = 1e9  # elastic
+    d.precision = precision
+    sign = -1.0 if corner == "low" else 1.0
+    vel = np.tile(sign * speed * np.array([1.0, 0.7, 0.4]), (len(pos), 1))
+    mass = np.full(len(pos), 1000.0 * d.particle_volume)
+    return SceneSpec(f"wall_slide_{corner}", d, pos, mass, vel, mat, 20)
 
 
 def plates_sized(n_target: int, seed: int = 0, precision: int = G.PRECISION_FP32_FP64SVD, e_scale: float = 1.0,

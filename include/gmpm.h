@@ -48,7 +48,7 @@ typedef enum gmpm_status {
 #define GMPM_FLAG_OUT_OF_DOMAIN   0x1u
 #define GMPM_FLAG_NONFINITE       0x2u
 #define GMPM_FLAG_SVD_NOCONVERGE  0x4u
-#define GMPM_FLAG_TABLE_OVERFLOW  0x8u   /* page capacity exceeded, or a cell above 4096 particles
+#define GMPM_FLAG_TABLE_OVERFLOW  0x8u   /* page capacity exceeded, or a cell above 6144 particles
                                             (that cell then keeps a non-canonical order) */
 #define GMPM_FLAG_COPY_TIMEOUT    0x10u  /* an asynchronous copy did not complete within the kernel's bounded
                                             wait; the kernel stopped early (reported as GMPM_CUDA_ERROR) */
@@ -350,8 +350,13 @@ const char* gmpm_status_string(gmpm_status status);
  * Outputs: perm[i] = input index of sorted slot i and keys_sorted[i] =
  * (page_key << 6) | cell, identical to GMPM_BIN_PERM / GMPM_BIN_KEYS of a scene
  * holding the same positions in the same order (stable sort by key).
- * Positions whose stencil leaves the grid are clamped as in the scene binning;
- * no flag is reported.  The call is asynchronous on `stream`.
+ * flags (device pointer, may be NULL) receives the call's GMPM_FLAG_* bits:
+ * GMPM_FLAG_OUT_OF_DOMAIN when a position's stencil left the grid (it is then
+ * clamped as in the scene binning), GMPM_FLAG_TABLE_OVERFLOW when a cell holds
+ * more than 6144 particles (only clamped positions pile up like that); such a
+ * cell keeps its scatter order, which can differ from run to run, while every
+ * other cell is in canonical order.  The call is asynchronous on `stream`,
+ * which must belong to the current device.
  *
  * Limits: n <= GMPM_NOALLOC_MAX_PARTICLES and 8 <= res <= GMPM_NOALLOC_MAX_RES
  * per axis; anything larger returns GMPM_INVALID_ARG before any work.
@@ -360,12 +365,13 @@ const char* gmpm_status_string(gmpm_status status);
  * it: calls that overlap on the GPU (different streams, or threads without
  * ordering) race and must be serialised by the caller.  The first call on a
  * device resolves the array's address with cudaGetSymbolAddress; make that
- * first call before any stream capture. */
+ * first call before any stream capture.  The returned status is that of this
+ * call's own API calls and launches. */
 #define GMPM_NOALLOC_MAX_PARTICLES 1048576
 #define GMPM_NOALLOC_MAX_RES 128
 #define GMPM_NOALLOC_SCRATCH_BYTES 21269248
 gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_t n, double dx, int res_x, int res_y, int res_z,
-                                       int32_t* perm, uint32_t* keys_sorted, void* stream);
+                                       int32_t* perm, uint32_t* keys_sorted, uint32_t* flags, void* stream);
 
 /* ---- synthetic scenes (host only, no device needed) ----------------------- */
 

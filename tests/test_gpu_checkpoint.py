@@ -54,3 +54,28 @@ def test_load_rejects_bad_files(pkg, ctx, tmp_path):
     with pytest.raises(G.GmpmError) as e:
         G.Scene.load(ctx, bad)
     assert e.value.status == G.IO_ERROR
+
+
+def test_load_rejects_other_format_versions_and_precisions(pkg, ctx, tmp_path):
+    """A valid file with its format version (uint32 at byte 8) or its real
+    size (uint32 at byte 12) changed is refused: a file from a build with
+    another particle layout must not be read as this one's."""
+    G = pkg.gmpm
+    sc = pkg.scenes.notched_bar(cells=(8, 8, 16), res=32, dx=1.0 / 32).build(ctx)
+    sc.substep(2)
+    good = tmp_path / "good.gmpm"
+    sc.save(good)
+    sc.close()
+    G.Scene.load(ctx, good).close()  # the unchanged file loads
+    data = bytearray(good.read_bytes())
+    version = int.from_bytes(data[8:12], "little")
+    real_bytes = int.from_bytes(data[12:16], "little")
+    assert version >= 2 and real_bytes in (4, 8)
+    for offset, value in ((8, version - 1), (8, version + 1), (12, 12 - real_bytes)):
+        bad = bytearray(data)
+        bad[offset:offset + 4] = int(value).to_bytes(4, "little")
+        path = tmp_path / f"patched_{offset}_{value}.gmpm"
+        path.write_bytes(bytes(bad))
+        with pytest.raises(G.GmpmError) as e:
+            G.Scene.load(ctx, path)
+        assert e.value.status == G.IO_ERROR, (offset, value)
