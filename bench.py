@@ -81,33 +81,40 @@ def measured_traffic() -> dict:
     return {}
 
 
+WORKLOADS = {
+    "plates_33m": "plates_33m: 4 plates of 256x256x16 cells, dx=1/256, 8 ppc, sphere impactor r=0.1 at 5 m/s, "
+                  "g=-9.8, dt=5e-5",
+    "plates_8m": "plates_8m: 4 plates of 128x128x16 cells, dx=1/128, 8 ppc, sphere impactor r=0.1 at 5 m/s, "
+                 "g=-9.8, dt=5e-5",
+    "notched_bar": "notched_bar: 16x16x64 cells, dx=1/128, 8 ppc, pulled at +/-0.5 m/s, dt=1e-4",
+}
+
+
 def workload(pkg, name: str, seed: int = 0):
     S = pkg.scenes
-    if name == "plates_33m":
-        return S.plates(seed=seed), ("plates_33m: 4 plates of 256x256x16 cells, dx=1/256, 8 ppc, "
-                                     "sphere impactor r=0.1 at 5 m/s, g=-9.8, dt=5e-5")
-    if name == "plates_8m":
-        return S.plates_8m(seed=seed), ("plates_8m: 4 plates of 128x128x16 cells, dx=1/128, 8 ppc, "
-                                        "sphere impactor r=0.1 at 5 m/s, g=-9.8, dt=5e-5")
-    if name == "notched_bar":
-        return S.notched_bar(seed=seed), ("notched_bar: 16x16x64 cells, dx=1/128, 8 ppc, pulled at +/-0.5 m/s, "
-                                          "dt=1e-4")
-    raise SystemExit(f"unknown workload {name}")
+    make = {"plates_33m": S.plates, "plates_8m": S.plates_8m, "notched_bar": S.notched_bar}.get(name)
+    if make is None:
+        raise SystemExit(f"unknown workload {name}")
+    return make(seed=seed), WORKLOADS[name]
 
 
-def cpu_sample(pkg, name: str):
+def cpu_sample(pkg, oracle, name: str):
+    """The CPU legs' sample of the workload, set up through the oracle (the
+    same description and particles as the library's set-up), so that these
+    legs do not load the product library."""
     S = pkg.scenes
+    setup = oracle.SceneSetup(pkg.gmpm)
     if name.startswith("plates"):
         dx = 1.0 / 256 if name == "plates_33m" else 1.0 / 128
         sp = S._plate_scene("plates_sample", CPU_SAMPLE_CELLS, dx, 8, 8, 8 if dx < 1 / 200 else 4,
-                            160 if dx < 1 / 200 else 96, 0, pkg.gmpm.PRECISION_FP64, 10)
+                            160 if dx < 1 / 200 else 96, 0, pkg.gmpm.PRECISION_FP64, 10, setup=setup)
         return sp, f"4 plates of {CPU_SAMPLE_CELLS}x{CPU_SAMPLE_CELLS}x16 cells (same dx, ppc, materials), {sp.n} particles"
-    sp = S.notched_bar(precision=pkg.gmpm.PRECISION_FP64)
+    sp = S.notched_bar(precision=pkg.gmpm.PRECISION_FP64, setup=setup)
     return sp, f"the full notched bar, {sp.n} particles"
 
 
 def time_oracle(pkg, oracle, name: str, steps: int, warmup: int, budget_s: float | None = None):
-    sp, what = cpu_sample(pkg, name)
+    sp, what = cpu_sample(pkg, oracle, name)
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     o = oracle.OracleScene(sp.desc, sp.positions, sp.masses, sp.velocities, sp.material_ids)
@@ -463,8 +470,10 @@ def main():
         if rank != 0:
             return
         oracle = load_oracle()
+        if args.workload not in WORKLOADS:
+            raise SystemExit(f"unknown workload {args.workload}")
         r = time_oracle(pkg, oracle, args.workload, args.steps, args.warmup)
-        sp, what = workload(pkg, args.workload)
+        what = WORKLOADS[args.workload]
         line = dict(metric="particle-substeps/sec", value=r["value"], unit="particle-substeps/s", n_gpus=0,
                     steps=args.steps, warmup=args.warmup, ms_per_step=r["ms_per_step"], higher_is_better=True,
                     scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",

@@ -61,14 +61,15 @@ def config_material(m: G.Material, dx: float, E: float = 1e5) -> None:
 
 def notched_bar(seed: int = 0, precision: int = G.PRECISION_FP32, cells=(16, 16, 64), ppc: int = 8,
                 dx: float = 1.0 / 128, pull: float = 0.5, notch=(1, 4), res: int = 128,
-                substeps: int = 500) -> SceneSpec:
-    """Notched bar along z, gripped over 2 cells at each end and pulled apart."""
+                substeps: int = 500, setup=G) -> SceneSpec:
+    """Notched bar along z, gripped over 2 cells at each end and pulled apart.
+    setup: as for the plate scenes."""
     nx, ny, nz = cells
     origin = ((res - nx) // 2 * dx, (res - ny) // 2 * dx, (res - nz) // 2 * dx)
     geom = G.Geometry(kind=0, cells=(nx, ny, nz), ppc=ppc, n_plates=1, gap_cells=0, notch_width=notch[0],
                       notch_depth=notch[1], dx=dx, origin=origin, seed=seed)
-    pos, mat = G.generate_particles(geom)
-    d = G.reference_defaults(dx, (res, res, res))
+    pos, mat = setup.generate_particles(geom)
+    d = setup.reference_defaults(dx, (res, res, res))
     d.dt = 1e-4
     d.gravity[0] = d.gravity[1] = d.gravity[2] = 0.0
     d.particle_volume = dx ** 3 / ppc
@@ -120,15 +121,18 @@ def notched_bar_batch(n_scenes: int = 64, seed: int = 0, lo: int = 10_000, hi: i
 
 
 def _plate_scene(name: str, cells_xy: int, dx: float, ppc: int, margin: int, gap: int, res_y: int, seed: int,
-                 precision: int, substeps: int, sphere_gap: float = 2.0) -> SceneSpec:
+                 precision: int, substeps: int, sphere_gap: float = 2.0, setup=G) -> SceneSpec:
+    """setup: provides generate_particles(geometry) and reference_defaults(dx,
+    res); this module's library binding unless a caller that must not load the
+    library passes another implementation of the same two functions."""
     n_plates = 4
     thick = 16
     res_xz = cells_xy + 2 * margin
     origin = (margin * dx, margin * dx, margin * dx)
     geom = G.Geometry(kind=1, cells=(cells_xy, thick, cells_xy), ppc=ppc, n_plates=n_plates, gap_cells=gap,
                       notch_width=0, notch_depth=0, dx=dx, origin=origin, seed=seed)
-    pos, mat = G.generate_particles(geom)
-    d = G.reference_defaults(dx, (res_xz, res_y, res_xz))
+    pos, mat = setup.generate_particles(geom)
+    d = setup.reference_defaults(dx, (res_xz, res_y, res_xz))
     d.dt = 5e-5
     d.gravity[0], d.gravity[1], d.gravity[2] = 0.0, -9.8, 0.0
     d.particle_volume = dx ** 3 / ppc

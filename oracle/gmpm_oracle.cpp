@@ -1603,4 +1603,96 @@ void orc_diagnostics(const orc_scene* s, gmpm_diag* d) {
     d->flags = s->flags;
 }
 
+// ---- scene set-up for the CPU legs that must not load the product library ----
+
+// The reference's compile-time configuration as a scene description: the
+// constants of Setting.h, Simulator.cpp and applyVonMises with a caller-chosen
+// grid (the same values the library's gmpm_scene_desc_reference_defaults sets).
+int orc_scene_desc_reference_defaults(gmpm_scene_desc* d, double dx, int rx, int ry, int rz) {
+    if (!d || !(dx > 0)) return GMPM_INVALID_ARG;
+    std::memset(d, 0, sizeof(*d));
+    d->dx = dx;
+    d->grid_res[0] = rx;
+    d->grid_res[1] = ry;
+    d->grid_res[2] = rz;
+    d->dt = 1e-4;                      // Simulator.cpp:172
+    d->gravity[1] = -10.0;             // TimeIntegrator.cu:100
+    d->particle_volume = dx * dx * dx / 8.0;
+    d->n_materials = 1;
+    gmpm_material& m = d->materials[0];
+    m.youngs_modulus = 2e2;            // Simulator.cpp:114-116
+    m.poisson_ratio = 0.4;
+    m.density = 3.0;
+    m.yield_stress = 800.0;            // ExplicitTimeIntegrator.cu:188
+    m.hardening_law = GMPM_HARDENING_EXPONENTIAL;
+    m.hardening = 3.0;                 // :189
+    m.alpha_cap = 1.0;                 // :194
+    m.dlambda_cap = 100.0;             // :217-220
+    m.strain_cap = 3.0;                // :267-271
+    m.psi_cap = 1e6;                   // :313
+    m.fracture_energy = 3.0;           // :317
+    m.softening_onset = 0.01;          // :320
+    m.residual_fracture = 0.1;         // :327
+    m.theta = (double)0.0001f;         // :334
+    m.length_scale = 0.5 * dx;         // :335
+    m.mobility = 50.0;                 // Materials.cpp:13
+    d->wall_bc = 1;
+    d->wall_layers = 4;                // TimeIntegrator.cu:134-164
+    d->precision = GMPM_PRECISION_FP32;
+    d->phase_field = GMPM_PHASE_FIELD_EXPLICIT;
+    d->deterministic = 1;
+    d->svd_fallback_ratio = 1e-3;
+    d->cfl_number = (double)0.3f;      // Simulator.cpp:211
+    d->pcg_max_iterations = 100;       // ExplicitTimeIntegrator.cu:925
+    d->pcg_tolerance = (double)1e-6f;  // :926
+    return GMPM_OK;
+}
+
+// Seeded particles of the synthetic scenes: every cell of the body gets ppc
+// positions drawn uniformly in the cell from one splitmix64 stream (each
+// draw's top 53 bits over 2^53), rounded to float, in the order plate, x
+// cell, y cell, z cell, particle, axis; the notch (kind 0) drops the cells of
+// notch_width z-indices centred at mid-length with y-index below notch_depth.
+int orc_generate_particles(const gmpm_scene_geometry* g, int64_t* count, double* positions, int32_t* material_ids,
+                           int64_t capacity) {
+    if (!g || !count || g->kind < 0 || g->kind > 2 || g->ppc <= 0 || !(g->dx > 0)) return GMPM_INVALID_ARG;
+    const int plates = g->kind == 1 ? g->n_plates : 1;
+    if (plates <= 0 || g->cells[0] <= 0 || g->cells[1] <= 0 || g->cells[2] <= 0) return GMPM_INVALID_ARG;
+    auto notch = [&](int iy, int iz) {
+        if (g->kind != 0 || g->notch_width <= 0 || g->notch_depth <= 0) return false;
+        const int z0 = g->cells[2] / 2 - g->notch_width / 2;
+        return iz >= z0 && iz < z0 + g->notch_width && iy < g->notch_depth;
+    };
+    int64_t per_plate = 0;
+    for (int iy = 0; iy < g->cells[1]; ++iy)
+        for (int iz = 0; iz < g->cells[2]; ++iz)
+            if (!notch(iy, iz)) per_plate += (int64_t)g->cells[0] * g->ppc;
+    *count = per_plate * plates;
+    if (!positions) return GMPM_OK;
+    if (capacity < *count) return GMPM_INVALID_ARG;
+    uint64_t state = g->seed;
+    auto draw = [&state]() {
+        state += 0x9e3779b97f4a7c15ull;
+        uint64_t z = state;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        z ^= z >> 31;
+        return (double)(z >> 11) / 9007199254740992.0;
+    };
+    int64_t p = 0;
+    for (int k = 0; k < plates; ++k)
+        for (int ix = 0; ix < g->cells[0]; ++ix)
+            for (int iy = 0; iy < g->cells[1]; ++iy)
+                for (int iz = 0; iz < g->cells[2]; ++iz) {
+                    if (notch(iy, iz)) continue;
+                    const int cell[3] = {ix, iy + k * (g->cells[1] + g->gap_cells), iz};
+                    for (int q = 0; q < g->ppc; ++q, ++p) {
+                        for (int a = 0; a < 3; ++a)
+                            positions[3 * p + a] = (double)(float)(g->origin[a] + (cell[a] + draw()) * g->dx);
+                        if (material_ids) material_ids[p] = k;
+                    }
+                }
+    return GMPM_OK;
+}
+
 }  // extern "C"

@@ -63,6 +63,14 @@ int orc_base_node(double inv_dx, const int32_t res[3], const double x[3], int32_
  * out: velocity xyz, c = sum w c / sum w (FP64 division). */
 void orc_grid_node(const gmpm_scene_desc* desc, double t, const int32_t node[3], const double ch[9], double out[4]);
 
+/* Scene set-up without the product library (the CPU legs of the benchmark):
+ * the reference-default description and the seeded synthetic particles, equal
+ * field for field and bit for bit to gmpm_scene_desc_reference_defaults and
+ * gmpm_generate_particles. */
+int orc_scene_desc_reference_defaults(gmpm_scene_desc* d, double dx, int rx, int ry, int rz);
+int orc_generate_particles(const gmpm_scene_geometry* g, int64_t* count, double* positions, int32_t* material_ids,
+                           int64_t capacity);
+
 typedef struct orc_scene orc_scene;
 
 orc_scene* orc_scene_create(const gmpm_scene_desc* desc, int64_t n, const double* pos,

@@ -48,6 +48,10 @@ def lib(desc_type=None, diag_type=None, material_type=None) -> C.CDLL:
         L.orc_base_node.restype = C.c_int
         L.orc_base_node.argtypes = [C.c_double, ip, dp, ip]
         L.orc_grid_node.argtypes = [vp, C.c_double, ip, dp, dp]
+        L.orc_scene_desc_reference_defaults.restype = C.c_int
+        L.orc_scene_desc_reference_defaults.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int]
+        L.orc_generate_particles.restype = C.c_int
+        L.orc_generate_particles.argtypes = [vp, C.POINTER(C.c_int64), dp, ip, C.c_int64]
         L.orc_scene_create.restype = vp
         L.orc_scene_create.argtypes = [vp, C.c_int64, dp, dp, dp, ip]
         L.orc_scene_destroy.argtypes = [vp]
@@ -140,3 +144,30 @@ def set_threads(n: int) -> None:
 
 def get_threads() -> int:
     return int(lib().orc_get_threads())
+
+
+class SceneSetup:
+    """Scene set-up through the oracle instead of the product library, for the
+    benchmark's CPU legs: the same ctypes structures (pure Python) filled by
+    orc_scene_desc_reference_defaults and orc_generate_particles."""
+
+    def __init__(self, G):
+        self.G = G  # the package's gmpm module (its structure types only)
+
+    def reference_defaults(self, dx: float, res):
+        d = self.G.SceneDesc()
+        if lib().orc_scene_desc_reference_defaults(C.byref(d), dx, int(res[0]), int(res[1]), int(res[2])) != 0:
+            raise RuntimeError("orc_scene_desc_reference_defaults failed")
+        return d
+
+    def generate_particles(self, geom):
+        L = lib()
+        n = C.c_int64(0)
+        if L.orc_generate_particles(C.byref(geom), C.byref(n), None, None, 0) != 0:
+            raise RuntimeError("orc_generate_particles failed")
+        pos = np.empty((n.value, 3), dtype=np.float64)
+        mat = np.empty(n.value, dtype=np.int32)
+        if L.orc_generate_particles(C.byref(geom), C.byref(n), _dptr(pos), mat.ctypes.data_as(C.POINTER(C.c_int32)),
+                                    n.value) != 0:
+            raise RuntimeError("orc_generate_particles failed")
+        return pos, mat

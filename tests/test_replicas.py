@@ -97,3 +97,39 @@ def test_reference_arm_line_contract():
     assert cpu["sample"]
     assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_does_not_load_the_product_library():
+    """The reference arm sets its sample up through the oracle, so the process
+    maps oracle/liboracle.so and never the library under test."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1'];\n"
+            "runpy.run_path('bench.py', run_name='__main__')\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('LIBGMPM', 'libgmpm.so' in maps, 'LIBORACLE', 'liboracle.so' in maps)")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "LIBGMPM False LIBORACLE True" in r.stdout, r.stdout[-500:]
+
+
+def test_oracle_scene_setup_equals_the_librarys(pkg, oracle):
+    """The CPU legs' set-up (oracle) gives the library's scene description
+    byte for byte and its seeded particles bit for bit."""
+    import ctypes as C
+
+    import numpy as np
+
+    G = pkg.gmpm
+    setup = oracle.SceneSetup(G)
+    for dx, res in ((1.0 / 256, (272, 160, 272)), (1.0 / 128, (128, 128, 128))):
+        a, b = G.reference_defaults(dx, res), setup.reference_defaults(dx, res)
+        assert C.string_at(C.addressof(a), C.sizeof(a)) == C.string_at(C.addressof(b), C.sizeof(b))
+    geoms = [G.Geometry(kind=1, cells=(12, 16, 10), ppc=8, n_plates=4, gap_cells=8, notch_width=0, notch_depth=0,
+                        dx=1.0 / 256, origin=(8 / 256, 8 / 256, 8 / 256), seed=0),
+             G.Geometry(kind=0, cells=(16, 16, 64), ppc=8, n_plates=1, gap_cells=0, notch_width=1, notch_depth=4,
+                        dx=1.0 / 128, origin=(0.4375, 0.4375, 0.25), seed=3),
+             G.Geometry(kind=2, cells=(5, 7, 3), ppc=3, n_plates=1, gap_cells=0, notch_width=0, notch_depth=0,
+                        dx=1.0 / 64, origin=(0.25, 0.3, 0.35), seed=11)]
+    for g in geoms:
+        pa, ma = G.generate_particles(g)
+        pb, mb = setup.generate_particles(g)
+        assert np.array_equal(pa, pb) and np.array_equal(ma, mb)
