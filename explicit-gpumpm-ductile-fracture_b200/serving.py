@@ -2,6 +2,13 @@
 gmpm_server (continuous batching), with request latency percentiles and the
 aggregate particle-substeps/s.
 
+Latency is reported over every arrival, not only the requests that finished:
+a request still queued or running when the run ends is counted at its age
+then (a lower bound on its latency; "censored"), and one never submitted is
+counted at the time left after its arrival.  With drain_s > 0 the loop keeps
+stepping after the last arrival until every request has finished (or drain_s
+has passed), so that at a sustainable load no latency is censored.
+
 A producer thread generates each request (its particles are part of the
 request, not of the server's work) and submits it at its arrival time; the
 main thread advances the server in chunks of substeps and collects finished
@@ -93,14 +100,29 @@ def run_served(ctx: G.Context, duration_s: float = 600.0, rate_hz: float = 20.0,
                 pending.discard(rid)
         poll_s += time.perf_counter() - t2
     elapsed = time.perf_counter() - t0
+    # requests left at the end: their age on the server's clock (a lower bound on their latency)
+    ages = []
+    for rid in pending:
+        p = srv.poll(rid)
+        ages.append(max(0.0, elapsed - p["submit_time"]))
+    # arrivals the producer never submitted: the time since their arrival
+    ages += [max(0.0, elapsed - t_arr) for t_arr in arrivals[n_submitted:]]
     st = srv.stats()
     srv.close()
     lat = np.array([d["latency"] for d in done if d["ok"]]) if done else np.zeros(0)
+    everyone = np.concatenate([lat, np.array(ages)])
+
+    def pct(a, q):
+        return float(np.percentile(a, q)) if len(a) else None
+
     return dict(
         duration_s=elapsed, arrivals=len(arrivals), submitted=n_submitted, completed=int(sum(d["ok"] for d in done)),
-        failed=int(sum(not d["ok"] for d in done)), unfinished=len(pending),
-        p50_latency_s=float(np.percentile(lat, 50)) if len(lat) else None,
-        p99_latency_s=float(np.percentile(lat, 99)) if len(lat) else None,
+        failed=int(sum(not d["ok"] for d in done)), unfinished=len(ages),
+        p50_latency_s=pct(lat, 50), p99_latency_s=pct(lat, 99),
+        # over every arrival, unfinished ones censored at their age at the end (lower bounds)
+        p50_latency_all_s=pct(everyone, 50), p99_latency_all_s=pct(everyone, 99),
+        unfinished_age_p50_s=pct(np.array(ages), 50), unfinished_age_p99_s=pct(np.array(ages), 99),
+        censored_fraction=float(len(ages) / max(1, len(arrivals))),
         mean_queue_s=float(np.mean([d["queue"] for d in done])) if done else None,
         particle_substeps_per_s=st["particle_substeps"] / elapsed, batches=st["batches"],
         capture_s=st["capture_microseconds"] / 1e6, admit_s=st["admit_microseconds"] / 1e6,

@@ -60,3 +60,20 @@ def test_server_rejects_oversized_request(pkg, ctx):
     with pytest.raises(G.GmpmError):
         srv.submit_spec(sp, 10)
     srv.close()
+
+
+def test_served_driver_reports_every_arrival(pkg, ctx):
+    """The serving driver's latency covers every arrival: drained at a light
+    load nothing is censored; cut off under overload, the unfinished requests
+    are counted at their age at the end, so the all-arrival percentiles are
+    at least the completed-only ones."""
+    from gmpm_b200 import serving  # noqa: E402  (loaded by the pkg fixture)
+
+    light = serving.run_served(ctx, duration_s=2.0, rate_hz=3.0, seed=4, lo=20_000, hi=40_000, drain_s=60.0)
+    assert light["arrivals"] > 0 and light["completed"] == light["arrivals"] and light["unfinished"] == 0
+    assert light["censored_fraction"] == 0.0
+    assert light["p50_latency_all_s"] == pytest.approx(light["p50_latency_s"])
+    assert light["p99_latency_all_s"] == pytest.approx(light["p99_latency_s"])
+    heavy = serving.run_served(ctx, duration_s=2.0, rate_hz=40.0, seed=5, lo=200_000, hi=400_000)
+    assert heavy["unfinished"] > 0 and heavy["completed"] + heavy["unfinished"] + heavy["failed"] == heavy["arrivals"]
+    assert heavy["p99_latency_all_s"] >= heavy["unfinished_age_p50_s"] > 0
