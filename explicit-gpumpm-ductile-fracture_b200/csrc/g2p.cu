@@ -90,6 +90,185 @@ __device__ __forceinline__ void bspline1d_g(R xp, R inv_dx, R* w, R* g) {
     g[2] = z * inv_dx;
 }
 
+// Gather of v, dc, grad v, B and grad c over the particle's 3x3x3 stencil
+// (G2PKernal.cu:286-357, AxG2P_APIC :1085-1112) from the page's staged window
+// (li, lj, lk: the base node's offset in the window).  The weights are tensor
+// products w = X_i Y_j Z_k, and the APIC offset x_i - x_p splits per axis, so
+// the sums are taken one axis at a time: over k for each (i, j) column, then
+// over j, then over i.
+template <typename R>
+__device__ __forceinline__ void gather_stencil(const R (*__restrict__ win4)[4], const R* __restrict__ wincn, int li,
+                                               int lj, int lk, const R xp[3], R dx, const R wx[3], const R gx[3],
+                                               const R wy[3], const R gy[3], const R wz[3], const R gz[3], R vp[3],
+                                               R& dcp, R gv[9], R Bn[9], R gc[3]) {
+    vp[0] = vp[1] = vp[2] = dcp = R(0);
+    gc[0] = gc[1] = gc[2] = R(0);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) gv[q] = Bn[q] = R(0);
+    R wxd[3], wyd[3], wzd[3];  // weight x (node - particle) offset per axis
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        wxd[q] = wx[q] * (R(q) * dx - xp[0]);
+        wyd[q] = wy[q] * (R(q) * dx - xp[1]);
+        wzd[q] = wz[q] * (R(q) * dx - xp[2]);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        // sums over j for this i: T0 (Y Z), Ty (Y' Z), Tz (Y Z'), Tdy (Y d Z), Tdz (Y Z d)
+        R T0[3], Ty[3], Tz[3], Tdy[3], Tdz[3], Td = R(0), Tc0 = R(0), Tcy = R(0), Tcz = R(0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) T0[a] = Ty[a] = Tz[a] = Tdy[a] = Tdz[a] = R(0);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            // sums over k for column (i, j): Z0 (Z), Z1 (Z'), Z2 (Z d)
+            R Z0[3], Z1[3], Z2[3], Zd = R(0), C0 = R(0), C1 = R(0);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Z0[a] = Z1[a] = Z2[a] = R(0);
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+                const int node = (li + i) * 36 + (lj + j) * 6 + (lk + kk);
+                R nv[4];
+                if (sizeof(R) == 4) {
+                    *reinterpret_cast<float4*>(nv) = *reinterpret_cast<const float4*>(&win4[node][0]);
+                } else {
+                    *reinterpret_cast<double2*>(nv) = *reinterpret_cast<const double2*>(&win4[node][0]);
+                    *reinterpret_cast<double2*>(nv + 2) = *reinterpret_cast<const double2*>(&win4[node][2]);
+                }
+                const R ncn = wincn[node];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    Z0[a] += wz[kk] * nv[a];
+                    Z1[a] += gz[kk] * nv[a];
+                    Z2[a] += wzd[kk] * nv[a];
+                }
+                Zd += wz[kk] * nv[3];
+                C0 += wz[kk] * ncn;
+                C1 += gz[kk] * ncn;
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                T0[a] += wy[j] * Z0[a];
+                Ty[a] += gy[j] * Z0[a];
+                Tz[a] += wy[j] * Z1[a];
+                Tdy[a] += wyd[j] * Z0[a];
+                Tdz[a] += wy[j] * Z2[a];
+            }
+            Td += wy[j] * Zd;
+            Tc0 += wy[j] * C0;
+            Tcy += gy[j] * C0;
+            Tcz += wy[j] * C1;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            vp[a] += wx[i] * T0[a];
+            gv[a + 0] += gx[i] * T0[a];
+            gv[a + 3] += wx[i] * Ty[a];
+            gv[a + 6] += wx[i] * Tz[a];
+            Bn[a + 0] += wxd[i] * T0[a];
+            Bn[a + 3] += wx[i] * Tdy[a];
+            Bn[a + 6] += wx[i] * Tdz[a];
+        }
+        dcp += wx[i] * Td;
+        gc[0] += gx[i] * Tc0;
+        gc[1] += wx[i] * Tcy;
+        gc[2] += wx[i] * Tcz;
+    }
+}
+
+// FP32: the same sums, two channels per packed instruction (fma.rn.f32x2).
+// Every value is the same fused multiply-add, in the same order, as in the
+// scalar form; the window's (v0, v1) and (v2, dc) halves of each 16-byte node
+// word are the packed operands, the weights are broadcast to both halves.
+template <>
+__device__ __forceinline__ void gather_stencil<float>(const float (*__restrict__ win4)[4],
+                                                      const float* __restrict__ wincn, int li, int lj, int lk,
+                                                      const float xp[3], float dx, const float wx[3],
+                                                      const float gx[3], const float wy[3], const float gy[3],
+                                                      const float wz[3], const float gz[3], float vp[3], float& dcp,
+                                                      float gv[9], float Bn[9], float gc[3]) {
+    float wxd[3], wyd[3], wzd[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        wxd[q] = wx[q] * (float(q) * dx - xp[0]);
+        wyd[q] = wy[q] * (float(q) * dx - xp[1]);
+        wzd[q] = wz[q] * (float(q) * dx - xp[2]);
+    }
+    const float2 zero = make_float2(0.f, 0.f);
+    // accumulators: pairs of channels (x, y components), then the z component alone,
+    // or (z component, damage increment) where both take the same weight
+    float2 VP01 = zero, VP2D = zero, GV01 = zero, GV34 = zero, GV67 = zero, B01 = zero, B34 = zero, B67 = zero;
+    float gv2 = 0.f, gv5 = 0.f, gv8 = 0.f, b2 = 0.f, b5 = 0.f, b8 = 0.f, gc0 = 0.f, gc1 = 0.f, gc2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float2 T001 = zero, T02D = zero, Ty01 = zero, Tz01 = zero, Tdy01 = zero, Tdz01 = zero;
+        float Ty2 = 0.f, Tz2 = 0.f, Tdy2 = 0.f, Tdz2 = 0.f, Tc0 = 0.f, Tcy = 0.f, Tcz = 0.f;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            float2 Z001 = zero, Z02D = zero, Z101 = zero, Z201 = zero;
+            float Z12 = 0.f, Z22 = 0.f, C0 = 0.f, C1 = 0.f;
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+                const int node = (li + i) * 36 + (lj + j) * 6 + (lk + kk);
+                const float4 nv = *reinterpret_cast<const float4*>(&win4[node][0]);
+                const float2 n01 = make_float2(nv.x, nv.y), n2d = make_float2(nv.z, nv.w);
+                const float ncn = wincn[node];
+                const float2 W = make_float2(wz[kk], wz[kk]), G = make_float2(gz[kk], gz[kk]);
+                const float2 WD = make_float2(wzd[kk], wzd[kk]);
+                Z001 = __ffma2_rn(W, n01, Z001);
+                Z02D = __ffma2_rn(W, n2d, Z02D);
+                Z101 = __ffma2_rn(G, n01, Z101);
+                Z12 = __fmaf_rn(gz[kk], nv.z, Z12);
+                Z201 = __ffma2_rn(WD, n01, Z201);
+                Z22 = __fmaf_rn(wzd[kk], nv.z, Z22);
+                C0 = __fmaf_rn(wz[kk], ncn, C0);
+                C1 = __fmaf_rn(gz[kk], ncn, C1);
+            }
+            const float2 WY = make_float2(wy[j], wy[j]), GY = make_float2(gy[j], gy[j]);
+            const float2 WYD = make_float2(wyd[j], wyd[j]);
+            T001 = __ffma2_rn(WY, Z001, T001);
+            T02D = __ffma2_rn(WY, Z02D, T02D);
+            Ty01 = __ffma2_rn(GY, Z001, Ty01);
+            Ty2 = __fmaf_rn(gy[j], Z02D.x, Ty2);
+            Tz01 = __ffma2_rn(WY, Z101, Tz01);
+            Tz2 = __fmaf_rn(wy[j], Z12, Tz2);
+            Tdy01 = __ffma2_rn(WYD, Z001, Tdy01);
+            Tdy2 = __fmaf_rn(wyd[j], Z02D.x, Tdy2);
+            Tdz01 = __ffma2_rn(WY, Z201, Tdz01);
+            Tdz2 = __fmaf_rn(wy[j], Z22, Tdz2);
+            Tc0 = __fmaf_rn(wy[j], C0, Tc0);
+            Tcy = __fmaf_rn(gy[j], C0, Tcy);
+            Tcz = __fmaf_rn(wy[j], C1, Tcz);
+        }
+        const float2 WX = make_float2(wx[i], wx[i]), GX = make_float2(gx[i], gx[i]);
+        const float2 WXD = make_float2(wxd[i], wxd[i]);
+        VP01 = __ffma2_rn(WX, T001, VP01);
+        VP2D = __ffma2_rn(WX, T02D, VP2D);
+        GV01 = __ffma2_rn(GX, T001, GV01);
+        gv2 = __fmaf_rn(gx[i], T02D.x, gv2);
+        GV34 = __ffma2_rn(WX, Ty01, GV34);
+        gv5 = __fmaf_rn(wx[i], Ty2, gv5);
+        GV67 = __ffma2_rn(WX, Tz01, GV67);
+        gv8 = __fmaf_rn(wx[i], Tz2, gv8);
+        B01 = __ffma2_rn(WXD, T001, B01);
+        b2 = __fmaf_rn(wxd[i], T02D.x, b2);
+        B34 = __ffma2_rn(WX, Tdy01, B34);
+        b5 = __fmaf_rn(wx[i], Tdy2, b5);
+        B67 = __ffma2_rn(WX, Tdz01, B67);
+        b8 = __fmaf_rn(wx[i], Tdz2, b8);
+        gc0 = __fmaf_rn(gx[i], Tc0, gc0);
+        gc1 = __fmaf_rn(wx[i], Tcy, gc1);
+        gc2 = __fmaf_rn(wx[i], Tcz, gc2);
+    }
+    vp[0] = VP01.x; vp[1] = VP01.y; vp[2] = VP2D.x; dcp = VP2D.y;
+    gv[0] = GV01.x; gv[1] = GV01.y; gv[2] = gv2;
+    gv[3] = GV34.x; gv[4] = GV34.y; gv[5] = gv5;
+    gv[6] = GV67.x; gv[7] = GV67.y; gv[8] = gv8;
+    Bn[0] = B01.x; Bn[1] = B01.y; Bn[2] = b2;
+    Bn[3] = B34.x; Bn[4] = B34.y; Bn[5] = b5;
+    Bn[6] = B67.x; Bn[7] = B67.y; Bn[8] = b8;
+    gc[0] = gc0; gc[1] = gc1; gc[2] = gc2;
+}
+
 // Unit sequence of one CTA: slots [b T / C, (b + 1) T / C) of the T sorted
 // slots, C = gridDim.x, in units of up to kG2PUnit slots and kUnitPages pages.
 // Every thread runs the same iterator in step (it shuffles), so it is called
@@ -297,80 +476,9 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
             // tensor products w = X_i Y_j Z_k, and the APIC offset x_i - x_p
             // splits per axis, so the sums are taken one axis at a time: over
             // k for each (i, j) column, then over j, then over i.
-            R vp[3] = {R(0), R(0), R(0)}, dcp = R(0);
-            R gv[9], Bn[9], gc[3] = {R(0), R(0), R(0)};
-#pragma unroll
-            for (int q = 0; q < 9; ++q) gv[q] = Bn[q] = R(0);
-            R wxd[3], wyd[3], wzd[3];  // weight x (node - particle) offset per axis
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                wxd[q] = wx[q] * (R(q) * dx - xp[0]);
-                wyd[q] = wy[q] * (R(q) * dx - xp[1]);
-                wzd[q] = wz[q] * (R(q) * dx - xp[2]);
-            }
-            const R(*win4)[4] = S.win4[pseq % kWinRing];
-            const R* wincn = S.wincn[pseq % kWinRing];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                // sums over j for this i: T0 (Y Z), Ty (Y' Z), Tz (Y Z'), Tdy (Y d Z), Tdz (Y Z d)
-                R T0[3], Ty[3], Tz[3], Tdy[3], Tdz[3], Td = R(0), Tc0 = R(0), Tcy = R(0), Tcz = R(0);
-#pragma unroll
-                for (int a = 0; a < 3; ++a) T0[a] = Ty[a] = Tz[a] = Tdy[a] = Tdz[a] = R(0);
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    // sums over k for column (i, j): Z0 (Z), Z1 (Z'), Z2 (Z d)
-                    R Z0[3], Z1[3], Z2[3], Zd = R(0), C0 = R(0), C1 = R(0);
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) Z0[a] = Z1[a] = Z2[a] = R(0);
-#pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        const int node = (li + i) * 36 + (lj + j) * 6 + (lk + kk);
-                        R nv[4];
-                        if (sizeof(R) == 4) {
-                            *reinterpret_cast<float4*>(nv) = *reinterpret_cast<const float4*>(&win4[node][0]);
-                        } else {
-                            *reinterpret_cast<double2*>(nv) = *reinterpret_cast<const double2*>(&win4[node][0]);
-                            *reinterpret_cast<double2*>(nv + 2) = *reinterpret_cast<const double2*>(&win4[node][2]);
-                        }
-                        const R ncn = wincn[node];
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            Z0[a] += wz[kk] * nv[a];
-                            Z1[a] += gz[kk] * nv[a];
-                            Z2[a] += wzd[kk] * nv[a];
-                        }
-                        Zd += wz[kk] * nv[3];
-                        C0 += wz[kk] * ncn;
-                        C1 += gz[kk] * ncn;
-                    }
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        T0[a] += wy[j] * Z0[a];
-                        Ty[a] += gy[j] * Z0[a];
-                        Tz[a] += wy[j] * Z1[a];
-                        Tdy[a] += wyd[j] * Z0[a];
-                        Tdz[a] += wy[j] * Z2[a];
-                    }
-                    Td += wy[j] * Zd;
-                    Tc0 += wy[j] * C0;
-                    Tcy += gy[j] * C0;
-                    Tcz += wy[j] * C1;
-                }
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    vp[a] += wx[i] * T0[a];
-                    gv[a + 0] += gx[i] * T0[a];
-                    gv[a + 3] += wx[i] * Ty[a];
-                    gv[a + 6] += wx[i] * Tz[a];
-                    Bn[a + 0] += wxd[i] * T0[a];
-                    Bn[a + 3] += wx[i] * Tdy[a];
-                    Bn[a + 6] += wx[i] * Tdz[a];
-                }
-                dcp += wx[i] * Td;
-                gc[0] += gx[i] * Tc0;
-                gc[1] += wx[i] * Tcy;
-                gc[2] += wx[i] * Tcz;
-            }
+            R vp[3], dcp, gv[9], Bn[9], gc[3];
+            gather_stencil(S.win4[pseq % kWinRing], S.wincn[pseq % kWinRing], li, lj, lk, xp, dx, wx, gx, wy, gy,
+                           wz, gz, vp, dcp, gv, Bn, gc);
             // damage: irreversible (G2PKernal.cu:359-366)
             const R c_old = S.p[buf][P_C][t];
             const R c_new = fmax(fmin(c_old, c_old + dcp), R(0));
