@@ -224,6 +224,9 @@ def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
     if getattr(args, "implicit", False):
         sp.desc.phase_field = G.PHASE_FIELD_IMPLICIT
         what += ", implicit phase field (Jacobi-PCG, tol 1e-6, <= 100 iterations)"
+    if getattr(args, "atomic_p2g", False):
+        sp.desc.deterministic = 0
+        what += ", P2G node sums with shared-memory atomics (not bitwise reproducible)"
     t0 = time.perf_counter()
     scene = sp.build(ctx)
     build_s = time.perf_counter() - t0
@@ -467,6 +470,8 @@ def main():
                     help="the reference's implicit (Jacobi-PCG) phase field instead of the explicit update")
     ap.add_argument("--no-served", action="store_true", help="skip the served-workload object of the line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--atomic-p2g", action="store_true",
+                    help="P2G's fast mode (shared-memory atomics) instead of the fixed-order, reproducible sums")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -562,7 +567,8 @@ def main():
             metric="particle-substeps/sec", value=res["value"], unit="particle-substeps/s", n_gpus=world,
             steps=args.steps, warmup=args.warmup, ms_per_step=res["ms_max"] / args.steps, higher_is_better=True,
             scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
-            config=dict(workload=res["what"], particles_per_gpu=sp.n, precision="fp32", deterministic_p2g=True,
+            config=dict(workload=res["what"], particles_per_gpu=sp.n, precision="fp32",
+                        deterministic_p2g=not args.atomic_p2g,
                         parallelism=f"replicas x{world}" if world > 1 else "single scene",
                         l2="resident state larger than L2 (no flush needed)"),
             roofline=dict(bound="hbm", kernel=res["dom"], achieved=k["achieved_gbs"], peak=res["peaks"]["hbm_gbs"],

@@ -219,19 +219,33 @@ def plates_sized(n_target: int, seed: int = 0, precision: int = G.PRECISION_FP32
     return sp
 
 
-def served_request(rng: np.random.Generator, k: int, lo: int = 20_000, hi: int = 2_000_000) -> tuple[SceneSpec, int]:
-    """One request of the served workload: a notched bar or a plate impact
-    (50/50), size log-uniform in [lo, hi], horizon uniform in [200, 2000]
-    substeps, parameters within +/-50% of the notched bar's."""
+def served_request_params(rng: np.random.Generator, lo: int = 20_000, hi: int = 2_000_000) -> dict:
+    """The random draws of one request of the served workload (cheap; the
+    particles are generated by served_request_build): a notched bar or a plate
+    impact (50/50), size log-uniform in [lo, hi], horizon uniform in
+    [200, 2000] substeps, parameters within +/-50% of the notched bar's."""
     n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
     horizon = int(rng.integers(200, 2001))
     f = rng.uniform(0.5, 1.5, 3)
-    if rng.random() < 0.5:
-        sp = notched_bar_sized(n, seed=k, E=1e5 * f[0], yield_stress=200.0 * f[1], density=1000.0 * f[2],
-                               pull=float(rng.uniform(0.2, 1.0)), substeps=horizon)
+    bar = bool(rng.random() < 0.5)
+    pull = float(rng.uniform(0.2, 1.0)) if bar else None
+    return dict(n=n, horizon=horizon, f=f, bar=bar, pull=pull)
+
+
+def served_request_build(params: dict, k: int) -> tuple[SceneSpec, int]:
+    p = params
+    f = p["f"]
+    if p["bar"]:
+        sp = notched_bar_sized(p["n"], seed=k, E=1e5 * f[0], yield_stress=200.0 * f[1], density=1000.0 * f[2],
+                               pull=p["pull"], substeps=p["horizon"])
     else:
-        sp = plates_sized(n, seed=k, e_scale=float(f[0]), substeps=horizon)
-    return sp, horizon
+        sp = plates_sized(p["n"], seed=k, e_scale=float(f[0]), substeps=p["horizon"])
+    return sp, p["horizon"]
+
+
+def served_request(rng: np.random.Generator, k: int, lo: int = 20_000, hi: int = 2_000_000) -> tuple[SceneSpec, int]:
+    """One request of the served workload (served_request_params, then its particles)."""
+    return served_request_build(served_request_params(rng, lo, hi), k)
 
 
 def blob(n_side: int = 12, ppc: int = 8, seed: int = 3, precision: int = G.PRECISION_FP32, dx: float = 1.0 / 64,

@@ -2,12 +2,19 @@
 gmpm_server (continuous batching), with request latency percentiles and the
 aggregate particle-substeps/s.
 
-Latency is reported over every arrival, not only the requests that finished:
-a request still queued or running when the run ends is counted at its age
-then (a lower bound on its latency; "censored"), and one never submitted is
-counted at the time left after its arrival.  With drain_s > 0 the loop keeps
-stepping after the last arrival until every request has finished (or drain_s
-has passed), so that at a sustainable load no latency is censored.
+Latency is reported over every accepted arrival, not only the requests that
+finished: a request still queued or running when the run ends is counted at
+its age then (a lower bound on its latency; "censored"), and one never
+submitted is counted at the time left after its arrival.  With drain_s > 0
+the loop keeps stepping after the last arrival until every request has
+finished (or drain_s has passed), so that at a sustainable load no latency is
+censored.
+
+The queue is bounded (max_queue): an arrival that finds max_queue requests
+waiting is rejected and counted, as a server sheds load under overload.
+Every queued request holds its particle arrays in host memory, so without a
+bound an overloaded run grows without limit; a rejected request's particles
+are never generated.
 
 A producer thread generates each request (its particles are part of the
 request, not of the server's work) and submits it at its arrival time; the
@@ -28,7 +35,8 @@ from . import scenes as S
 
 def run_served(ctx: G.Context, duration_s: float = 600.0, rate_hz: float = 20.0, seed: int = 0,
                lo: int = 20_000, hi: int = 2_000_000, budget_bytes: int = 120 * 10**9, chunk: int = 20,
-               max_live: int = 64, stream: int | None = None, drain_s: float = 0.0) -> dict:
+               max_live: int = 64, stream: int | None = None, drain_s: float = 0.0,
+               max_queue: int = 256) -> dict:
     rng = np.random.default_rng(seed)
     # arrival times (Poisson process) over the run
     arrivals = []
@@ -42,16 +50,23 @@ def run_served(ctx: G.Context, duration_s: float = 600.0, rate_hz: float = 20.0,
     submitted: queue.Queue = queue.Queue()
     t0 = time.perf_counter()
     submit_s = [0.0]
+    rejected = [0]
 
     def produce():
-        # generates each request ahead of its arrival and submits it on time
-        # (the server accepts submissions while another thread steps it)
+        # draws each request, generates its particles if the queue has room when
+        # it arrives, and submits it on time (the server accepts submissions while
+        # another thread steps it)
         prng = np.random.default_rng(seed + 1)
         for k, t_arr in enumerate(arrivals):
-            sp, horizon = S.served_request(prng, k, lo, hi)
+            params = S.served_request_params(prng, lo, hi)
             wait = t_arr - (time.perf_counter() - t0)
             if wait > 0:
                 time.sleep(wait)
+            if max_queue > 0 and srv.stats()["queued"] >= max_queue:
+                rejected[0] += 1
+                submitted.put(-1)
+                continue
+            sp, horizon = S.served_request_build(params, k)
             t1 = time.perf_counter()
             rid = srv.submit_spec(sp, horizon)
             submit_s[0] += time.perf_counter() - t1
@@ -63,6 +78,7 @@ def run_served(ctx: G.Context, duration_s: float = 600.0, rate_hz: float = 20.0,
     pending = set()
     done = []
     n_submitted = 0
+    n_handled = 0  # arrivals the producer has submitted or rejected
     producer_done = False
     peak_queue = 0
     step_s = poll_s = 0.0
@@ -74,7 +90,9 @@ def run_served(ctx: G.Context, duration_s: float = 600.0, rate_hz: float = 20.0,
                 break
             if rid is None:
                 producer_done = True
-            else:
+                continue
+            n_handled += 1
+            if rid >= 0:
                 pending.add(rid)
                 n_submitted += 1
         now = time.perf_counter() - t0
@@ -105,8 +123,8 @@ def run_served(ctx: G.Context, duration_s: float = 600.0, rate_hz: float = 20.0,
     for rid in pending:
         p = srv.poll(rid)
         ages.append(max(0.0, elapsed - p["submit_time"]))
-    # arrivals the producer never submitted: the time since their arrival
-    ages += [max(0.0, elapsed - t_arr) for t_arr in arrivals[n_submitted:]]
+    # arrivals the producer had not reached: the time since their arrival
+    ages += [max(0.0, elapsed - t_arr) for t_arr in arrivals[n_handled:]]
     st = srv.stats()
     srv.close()
     lat = np.array([d["latency"] for d in done if d["ok"]]) if done else np.zeros(0)
@@ -116,13 +134,14 @@ def run_served(ctx: G.Context, duration_s: float = 600.0, rate_hz: float = 20.0,
         return float(np.percentile(a, q)) if len(a) else None
 
     return dict(
-        duration_s=elapsed, arrivals=len(arrivals), submitted=n_submitted, completed=int(sum(d["ok"] for d in done)),
-        failed=int(sum(not d["ok"] for d in done)), unfinished=len(ages),
+        duration_s=elapsed, arrivals=len(arrivals), submitted=n_submitted, rejected=rejected[0],
+        rejected_fraction=float(rejected[0] / max(1, len(arrivals))), max_queue=max_queue,
+        completed=int(sum(d["ok"] for d in done)), failed=int(sum(not d["ok"] for d in done)), unfinished=len(ages),
         p50_latency_s=pct(lat, 50), p99_latency_s=pct(lat, 99),
         # over every arrival, unfinished ones censored at their age at the end (lower bounds)
         p50_latency_all_s=pct(everyone, 50), p99_latency_all_s=pct(everyone, 99),
         unfinished_age_p50_s=pct(np.array(ages), 50), unfinished_age_p99_s=pct(np.array(ages), 99),
-        censored_fraction=float(len(ages) / max(1, len(arrivals))),
+        censored_fraction=float(len(ages) / max(1, len(arrivals) - rejected[0])),
         mean_queue_s=float(np.mean([d["queue"] for d in done])) if done else None,
         particle_substeps_per_s=st["particle_substeps"] / elapsed, batches=st["batches"],
         capture_s=st["capture_microseconds"] / 1e6, admit_s=st["admit_microseconds"] / 1e6,

@@ -75,5 +75,10 @@ def test_served_driver_reports_every_arrival(pkg, ctx):
     assert light["p50_latency_all_s"] == pytest.approx(light["p50_latency_s"])
     assert light["p99_latency_all_s"] == pytest.approx(light["p99_latency_s"])
     heavy = serving.run_served(ctx, duration_s=2.0, rate_hz=40.0, seed=5, lo=200_000, hi=400_000)
-    assert heavy["unfinished"] > 0 and heavy["completed"] + heavy["unfinished"] + heavy["failed"] == heavy["arrivals"]
+    assert heavy["unfinished"] > 0
+    assert heavy["completed"] + heavy["unfinished"] + heavy["failed"] + heavy["rejected"] == heavy["arrivals"]
     assert heavy["p99_latency_all_s"] >= heavy["unfinished_age_p50_s"] > 0
+    # a bounded queue sheds the arrivals that find it full, and counts them
+    shed = serving.run_served(ctx, duration_s=2.0, rate_hz=40.0, seed=6, lo=200_000, hi=400_000, max_queue=4)
+    assert shed["rejected"] > 0 and shed["submitted"] + shed["rejected"] <= shed["arrivals"]
+    assert shed["completed"] + shed["unfinished"] + shed["failed"] + shed["rejected"] == shed["arrivals"]
