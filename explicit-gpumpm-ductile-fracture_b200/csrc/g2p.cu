@@ -384,7 +384,12 @@ __device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int 
     }
 }
 
-template <typename R, bool kAnyModel>
+// kAnyModel: a material uses an energy model other than von Mises.
+// kFallback: the scene redoes the SVD and return map in FP64 for ill-conditioned F
+// (FP32 with the FP64 fallback).  The fallback's FP64 registers make the FP32
+// kernel spill (76-136 bytes at 128 registers), so scenes without it launch
+// the instantiation that leaves it out (126 registers, no spills).
+template <typename R, bool kAnyModel, bool kFallback>
 __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
     k_g2p(const SceneDev<R>* __restrict__ sc, const SceneDev<double>* __restrict__ sc64, PState<R> in,
           PState<R> out, PAux<R> aux, BinDev bin, const R* __restrict__ nodes, Counters* cnt) {
@@ -393,7 +398,7 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
     const int t = threadIdx.x;
     const int nb = min(cnt->n_blocks, bin.nb_cap);
     const R dx = sc->dx, inv_dx = sc->inv_dx, dt = sc->dt, V0 = sc->V0;
-    const bool fallback = sc->fp64_svd_fallback && sc64 != nullptr;
+    const bool fallback = kFallback && sc->fp64_svd_fallback && sc64 != nullptr;
     const R ratio = sc->svd_fallback_ratio;
     unsigned int flags = 0;
     double v2max = 0.0;  // max |v_p|^2 of this thread's particles (adaptive dt)
@@ -585,10 +590,17 @@ __global__ void k_advance_time(Counters* cnt, SceneDev<R>* sc, SceneDev<double>*
 
 template <typename R>
 cudaError_t prepare_g2p() {
-    const cudaError_t e =
-        cudaFuncSetAttribute(k_g2p<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(G2PShared<R>));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_g2p<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(G2PShared<R>));
+    const int smem = (int)sizeof(G2PShared<R>);
+    cudaError_t e = cudaFuncSetAttribute(k_g2p<R, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_g2p<R, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if constexpr (sizeof(R) == 4) {
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_g2p<R, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_g2p<R, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    }
+    return e;
 }
 template cudaError_t prepare_g2p<float>();
 template cudaError_t prepare_g2p<double>();
@@ -600,12 +612,21 @@ cudaError_t launch_g2p(const SceneDev<R>* sc, const SceneDev<double>* sc64, cons
     const int per_sm = sizeof(R) == 4 ? kG2PMinBlocks : 1;
     const int64_t units = (bin.n + kG2PUnit - 1) / kG2PUnit;
     const int ctas = (int)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)cfg.num_sms * per_sm));
-    if (cfg.other_models)
-        k_g2p<R, true><<<ctas, kG2PUnit, sizeof(G2PShared<R>), stream>>>(sc, fallback64, in, out, aux, bin,
-                                               reinterpret_cast<const R*>(grid.nodes), cnt);
-    else
-        k_g2p<R, false><<<ctas, kG2PUnit, sizeof(G2PShared<R>), stream>>>(sc, fallback64, in, out, aux, bin,
-                                               reinterpret_cast<const R*>(grid.nodes), cnt);
+    const R* nodes = reinterpret_cast<const R*>(grid.nodes);
+    const size_t smem = sizeof(G2PShared<R>);
+    // FP64 state needs no FP64 fallback; FP32 launches the fallback form only where the scene has it
+    const bool fb = sizeof(R) == 4 && fallback64 != nullptr;
+    if (cfg.other_models) {
+        if (fb)
+            k_g2p<R, true, (sizeof(R) == 4)><<<ctas, kG2PUnit, smem, stream>>>(sc, fallback64, in, out, aux, bin, nodes, cnt);
+        else
+            k_g2p<R, true, false><<<ctas, kG2PUnit, smem, stream>>>(sc, fallback64, in, out, aux, bin, nodes, cnt);
+    } else {
+        if (fb)
+            k_g2p<R, false, (sizeof(R) == 4)><<<ctas, kG2PUnit, smem, stream>>>(sc, fallback64, in, out, aux, bin, nodes, cnt);
+        else
+            k_g2p<R, false, false><<<ctas, kG2PUnit, smem, stream>>>(sc, fallback64, in, out, aux, bin, nodes, cnt);
+    }
     k_advance_time<R><<<1, 1, 0, stream>>>(cnt, const_cast<SceneDev<R>*>(sc), const_cast<SceneDev<double>*>(sc64));
     return cudaGetLastError();
 }

@@ -429,9 +429,22 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
         }
         __syncthreads();
         {
-            // chunk k+1: staging (the buffer is free now); chunk k+2: iterator step, descriptor and meta
+            // chunk k+1: staging (the buffer is free now); chunk k+2: iterator step, descriptor and meta.
+            // The staging copies are issued by the warp whose column holds the fewest of this chunk's
+            // particles, so that the issue delays the sweep least (each warp finds it the same way).
             const int n1 = S.chunk[m1][2];
-            if (t == 0 && n1 > 0) {
+            int issuer;
+            {
+                const int* cs = S.cs[m0];
+                const int c1 = c0 + n0;
+                const int lw = lane & 15;
+                const int lcx = lw >> 2, lcy = ((lw & 3) - lcx) & 3, lcb = lcx * 16 + lcy * 4;
+                int key = ((min(max(cs[lcb + 4], c0), c1) - min(max(cs[lcb], c0), c1)) << 4) | lw;
+#pragma unroll
+                for (int off = 8; off > 0; off >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, off));
+                issuer = key & 15;
+            }
+            if (warp == issuer && lane == 0 && n1 > 0) {
                 S.win[m1] = window_start<R, CH>(S.o[m1], n1, st.stride);
                 issue_staging(S, stage, S.win[m1], st, aux);
             }
