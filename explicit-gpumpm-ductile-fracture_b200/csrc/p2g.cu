@@ -290,6 +290,10 @@ struct P2GMeta {
     int64_t win[3];       // first previous slot of the chunk's staging window
     uint64_t bar;         // completion of the staging bulk copies
     int abort;            // a bounded wait gave up
+    // page flush: the column-sum offsets of window node n's terms, in summing order
+    // (cell column cx then cy ascending), and their count
+    uint16_t goff[kWindowNodes][9];
+    uint8_t gcnt[kWindowNodes];
 };
 
 // Start of the staging window of a chunk: the median over three particles of
@@ -374,6 +378,14 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
         int b0, s0, n0, l0, b1, s1, n1, l1;
         it.step(bin, nb, b0, s0, n0, l0);
         it.step(bin, nb, b1, s1, n1, l1);
+        if (t < kWindowNodes) {
+            const int na = t / 36, nbb = (t / 6) % 6, nc = t % 6;
+            int q = 0;
+            for (int cx = max(0, na - 2); cx <= min(3, na); ++cx)
+                for (int cy = max(0, nbb - 2); cy <= min(3, nbb); ++cy)
+                    S.goff[t][q++] = (uint16_t)(((cx * 4 + cy) * 9 + (na - cx) * 3 + (nbb - cy)) * kColAcc + nc * 9);
+            S.gcnt[t] = (uint8_t)q;
+        }
         if (t == 0) {
             S.chunk[0][0] = b0; S.chunk[0][1] = s0; S.chunk[0][2] = n0; S.chunk[0][3] = l0;
             S.chunk[1][0] = b1; S.chunk[1][1] = s1; S.chunk[1][2] = n1; S.chunk[1][3] = l1;
@@ -496,22 +508,34 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
         __syncthreads();
         R* out = tile + (int64_t)b0 * kP2GChannels * kWindowNodes;
         if (kDeterministic) {
-            // window node (a, b, c): sum over cell columns (cx, cy) with stencil
-            // column (a - cx, b - cy), cx then cy ascending, all channels at once
-            if (t < kWindowNodes) {
-                const int na = t / 36, nbb = (t / 6) % 6, nc = t % 6;
-                R sum[kP2GChannels], comp[kP2GChannels];
+            // tile value (ch, n): window node n = (a, b, c) sums cell columns (cx, cy) with stencil
+            // column (a - cx, b - cy), cx then cy ascending (compensated).  One (channel, node) sum per
+            // thread step over all threads: the sums are short dependent chains, so spreading them keeps
+            // every warp busy where one thread per node left most of the CTA waiting.
+            constexpr int kItems = (kP2GChannels * kWindowNodes + kP2GThreads - 1) / kP2GThreads;
+            int base[kItems], cnt[kItems];
+            R sum[kItems], comp[kItems];
 #pragma unroll
-                for (int ch = 0; ch < kP2GChannels; ++ch) sum[ch] = comp[ch] = R(0);
-                for (int cx = max(0, na - 2); cx <= min(3, na); ++cx)
-                    for (int cy = max(0, nbb - 2); cy <= min(3, nbb); ++cy) {
-                        const R* src =
-                            acc_smem + ((cx * 4 + cy) * 9 + (na - cx) * 3 + (nbb - cy)) * kColAcc + nc * 9;
+            for (int i = 0; i < kItems; ++i) {
+                const int w = t + i * kP2GThreads;
+                const int ch = w / kWindowNodes;
+                const int n = w - ch * kWindowNodes;
+                const bool ok = w < kP2GChannels * kWindowNodes;
+                base[i] = ok ? n * 9 : 0;
+                cnt[i] = ok ? S.gcnt[n] : 0;
+                sum[i] = comp[i] = R(0);
+                base[i] = (base[i] << 4) | ch;  // node's offset row and channel
+            }
 #pragma unroll
-                        for (int ch = 0; ch < kP2GChannels; ++ch) kahan_add(sum[ch], comp[ch], src[ch]);
-                    }
+            for (int q = 0; q < 9; ++q)
 #pragma unroll
-                for (int ch = 0; ch < kP2GChannels; ++ch) out[ch * kWindowNodes + t] = sum[ch];
+                for (int i = 0; i < kItems; ++i)
+                    if (q < cnt[i])
+                        kahan_add(sum[i], comp[i], acc_smem[(&S.goff[0][0])[(base[i] >> 4) + q] + (base[i] & 15)]);
+#pragma unroll
+            for (int i = 0; i < kItems; ++i) {
+                const int w = t + i * kP2GThreads;
+                if (w < kP2GChannels * kWindowNodes) out[w] = sum[i];
             }
         } else {
             for (int oi = t; oi < kP2GChannels * kWindowNodes; oi += kP2GThreads) out[oi] = acc_smem[oi];
