@@ -42,6 +42,10 @@ constexpr int kP2GWarps = 16;  // one per cell z-column (cx, cy)
 constexpr int kP2GThreads = 32 * kP2GWarps;
 constexpr int kColumns = 144;  // 16 cell z-columns x 9 stencil columns
 constexpr int kColAcc = 54;    // 6 z-nodes x 9 channels per stencil column
+// Page flush: column sums channel-major, [channel][stencil column (144)][z (6)], the channel stride padded
+// so that the three channel groups of a warp's stores fall in different banks.  A gather step of one
+// channel over consecutive window nodes then reads consecutive words.
+constexpr int kFlushChStride = kColumns * 6 + 8;
 constexpr int kRec = 44;       // words per staged particle record
 
 template <typename R> struct P2GChunk;
@@ -346,7 +350,7 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
           Counters* __restrict__ cnt) {
     constexpr int CH = P2GChunk<R>::value;
     constexpr int W = Staging<R>::W, WS = Staging<R>::WS;
-    static_assert(sizeof(R) * kColumns * kColAcc <= p2g_rec_bytes<R>(), "column sums fit the record buffer");
+    static_assert(sizeof(R) * kP2GChannels * kFlushChStride <= p2g_rec_bytes<R>(), "column sums fit the record buffer");
     static_assert(sizeof(R) * kP2GChannels * kWindowNodes <= p2g_rec_bytes<R>(), "tile fits the record buffer");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* recs = reinterpret_cast<R*>(smem_raw);                          // [CH][kRec] particle records
@@ -383,7 +387,7 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
             int q = 0;
             for (int cx = max(0, na - 2); cx <= min(3, na); ++cx)
                 for (int cy = max(0, nbb - 2); cy <= min(3, nbb); ++cy)
-                    S.goff[t][q++] = (uint16_t)(((cx * 4 + cy) * 9 + (na - cx) * 3 + (nbb - cy)) * kColAcc + nc * 9);
+                    S.goff[t][q++] = (uint16_t)(((cx * 4 + cy) * 9 + (na - cx) * 3 + (nbb - cy)) * 6 + nc);
             S.gcnt[t] = (uint8_t)q;
         }
         if (t == 0) {
@@ -497,7 +501,7 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
 #pragma unroll
                 for (int z = 0; z < 6; ++z) {
                     if (kDeterministic)
-                        acc_smem[((wcx * 4 + wcy) * 9 + col) * kColAcc + z * 9 + ch] = acc[3 * z + q];
+                        acc_smem[ch * kFlushChStride + ((wcx * 4 + wcy) * 9 + col) * 6 + z] = acc[3 * z + q];
                     else
                         atomicAdd(&acc_smem[ch * kWindowNodes + a * 36 + bb * 6 + z], acc[3 * z + q]);
                 }
@@ -531,7 +535,8 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
 #pragma unroll
                 for (int i = 0; i < kItems; ++i)
                     if (q < cnt[i])
-                        kahan_add(sum[i], comp[i], acc_smem[(&S.goff[0][0])[(base[i] >> 4) + q] + (base[i] & 15)]);
+                        kahan_add(sum[i], comp[i],
+                                  acc_smem[(base[i] & 15) * kFlushChStride + (&S.goff[0][0])[(base[i] >> 4) + q]]);
 #pragma unroll
             for (int i = 0; i < kItems; ++i) {
                 const int w = t + i * kP2GThreads;
