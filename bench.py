@@ -113,8 +113,21 @@ def cpu_sample(pkg, oracle, name: str):
     return sp, f"the full notched bar, {sp.n} particles"
 
 
-def time_oracle(pkg, oracle, name: str, steps: int, warmup: int, budget_s: float | None = None):
-    sp, what = cpu_sample(pkg, oracle, name)
+def full_sample(pkg, oracle, name: str):
+    """The whole workload (the same scene as the CUDA arm, in FP64), set up through the oracle."""
+    S = pkg.scenes
+    setup = oracle.SceneSetup(pkg.gmpm)
+    make = {"plates_33m": S.plates, "plates_8m": S.plates_8m, "notched_bar": S.notched_bar}[name]
+    sp = make(precision=pkg.gmpm.PRECISION_FP64, setup=setup)
+    return sp, f"the full workload, {sp.n} particles"
+
+
+def time_oracle(pkg, oracle, name: str, steps: int, warmup: int, budget_s: float | None = None,
+                full: bool = False):
+    """Substeps of the oracle on all host cores.  full: the whole workload,
+    with the number of timed substeps cut to what fits in budget_s (each
+    substep is the whole workload, so the rate stays per substep)."""
+    sp, what = full_sample(pkg, oracle, name) if full else cpu_sample(pkg, oracle, name)
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     o = oracle.OracleScene(sp.desc, sp.positions, sp.masses, sp.velocities, sp.material_ids)
@@ -130,7 +143,7 @@ def time_oracle(pkg, oracle, name: str, steps: int, warmup: int, budget_s: float
     total = sum(per)
     return dict(value=sp.n * len(per) / total, unit="particle-substeps/s", cores=oracle.get_threads(),
                 kind="port", sample=f"{what}; {len(per)} substeps after {warmup} warm-up",
-                ms_per_step=1e3 * total / len(per))
+                ms_per_step=1e3 * total / len(per), timed_steps=len(per), particles=sp.n)
 
 
 class ClockSampler:
@@ -470,6 +483,8 @@ def main():
                     help="the reference's implicit (Jacobi-PCG) phase field instead of the explicit update")
     ap.add_argument("--no-served", action="store_true", help="skip the served-workload object of the line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-sample", action="store_true",
+                    help="reference arm: time the bounded CPU sample instead of the whole workload")
     ap.add_argument("--atomic-p2g", action="store_true",
                     help="P2G's fast mode (shared-memory atomics) instead of the fixed-order, reproducible sums")
     args = ap.parse_args()
@@ -487,12 +502,17 @@ def main():
         oracle = load_oracle()
         if args.workload not in WORKLOADS:
             raise SystemExit(f"unknown workload {args.workload}")
-        r = time_oracle(pkg, oracle, args.workload, args.steps, args.warmup)
+        # the whole workload (same configuration as the CUDA arm); timed substeps bounded so the run
+        # ends within a few minutes, or the bounded sample with --reference-sample
+        r = time_oracle(pkg, oracle, args.workload, args.steps, args.warmup,
+                        budget_s=None if args.reference_sample else 120.0, full=not args.reference_sample)
         what = WORKLOADS[args.workload]
         line = dict(metric="particle-substeps/sec", value=r["value"], unit="particle-substeps/s", n_gpus=0,
                     steps=args.steps, warmup=args.warmup, ms_per_step=r["ms_per_step"], higher_is_better=True,
                     scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-                    config=dict(workload=what, sample=r["sample"]), impl="reference",
+                    config=dict(workload=what, sample=r["sample"], particles=r["particles"],
+                                same_config=not args.reference_sample, timed_steps=r["timed_steps"]),
+                    impl="reference",
                     cpu_baseline=dict(value=r["value"], unit=r["unit"], cores=r["cores"], kind=r["kind"],
                                       sample=r["sample"]),
                     e2e=dict(value=r["value"], unit=r["unit"], h2d_bytes_per_step=0, d2h_bytes_per_step=0))

@@ -157,14 +157,14 @@ def _plate_scene(name: str, cells_xy: int, dx: float, ppc: int, margin: int, gap
     return SceneSpec(name, d, pos, mass, vel, mat, substeps)
 
 
-def plates(seed: int = 0, precision: int = G.PRECISION_FP32, substeps: int = 2000) -> SceneSpec:
+def plates(seed: int = 0, precision: int = G.PRECISION_FP32, substeps: int = 2000, setup=G) -> SceneSpec:
     """4 plates of 256x256x16 cells at dx=1/256, 8 ppc: 33,554,432 particles."""
-    return _plate_scene("plates_33m", 256, 1.0 / 256, 8, 8, 8, 160, seed, precision, substeps)
+    return _plate_scene("plates_33m", 256, 1.0 / 256, 8, 8, 8, 160, seed, precision, substeps, setup=setup)
 
 
-def plates_8m(seed: int = 0, precision: int = G.PRECISION_FP32, substeps: int = 100) -> SceneSpec:
+def plates_8m(seed: int = 0, precision: int = G.PRECISION_FP32, substeps: int = 100, setup=G) -> SceneSpec:
     """4 plates of 128x128x16 cells at dx=1/128, 8 ppc: 8,388,608 particles."""
-    return _plate_scene("plates_8m", 128, 1.0 / 128, 8, 8, 4, 96, seed, precision, substeps)
+    return _plate_scene("plates_8m", 128, 1.0 / 128, 8, 8, 4, 96, seed, precision, substeps, setup=setup)
 
 
 def plates_small(cells_xy: int = 32, seed: int = 0, precision: int = G.PRECISION_FP32,

@@ -84,7 +84,8 @@ def test_reference_arm_line_contract():
     and e2e objects that repeat the line's own value with no transfers."""
     env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
     r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "1"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+                        "--warmup", "1", "--reference-sample"], cwd=ROOT, env=env, capture_output=True, text=True,
+                       timeout=600)
     assert r.returncode == 0, r.stderr
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference"
@@ -97,12 +98,27 @@ def test_reference_arm_line_contract():
     assert cpu["sample"]
     assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    assert line["config"]["same_config"] is False
+
+
+def test_reference_arm_times_the_whole_workload():
+    """By default the reference arm runs the CUDA arm's own scene (here the
+    notched bar, small enough for a CPU test), not a sample of it."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload", "notched_bar",
+                        "--steps", "2", "--warmup", "3"], cwd=ROOT, env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["config"]["same_config"] is True and line["config"]["timed_steps"] == 2
+    assert line["config"]["particles"] == 130_560  # the notched bar, notch removed
+    assert line["config"]["workload"].startswith("notched_bar: 16x16x64 cells")
 
 
 def test_reference_arm_does_not_load_the_product_library():
     """The reference arm sets its sample up through the oracle, so the process
     maps oracle/liboracle.so and never the library under test."""
-    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1'];\n"
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--reference-sample'];\n"
             "runpy.run_path('bench.py', run_name='__main__')\n"
             "maps = open('/proc/self/maps').read()\n"
             "print('LIBGMPM', 'libgmpm.so' in maps, 'LIBORACLE', 'liboracle.so' in maps)")
