@@ -380,6 +380,7 @@ def run_batched(pkg, local_rank: int, steps: int, plain_steps: int, n_scenes: in
     batch.substep(tune + 2, sh)
     torch.cuda.synchronize(dev)
     info = batch.info()
+    # the scenes' own launches (branch scenes) plus the batch's launches over many scenes
     launches0 = sum(sc.diagnostics()["kernel_launches"] for sc in scenes)
     with ClockSampler(local_rank) as clocks:
         clocks.mark("t0")
@@ -389,7 +390,9 @@ def run_batched(pkg, local_rank: int, steps: int, plain_steps: int, n_scenes: in
         e1.synchronize()
         clocks.mark("t1")
     b_ms = e0.elapsed_time(e1)
-    launches = sum(sc.diagnostics()["kernel_launches"] for sc in scenes) - launches0
+    info = batch.info()
+    own = sum(sc.diagnostics()["kernel_launches"] for sc in scenes) - launches0
+    launches = own if info["table_scenes"] == 0 else info["kernel_nodes"] * steps
     status = max(sc.sync() for sc in scenes)
     batch.close()
     for sc in scenes:
@@ -573,7 +576,8 @@ def main():
         batched = {k: b[k] for k in ("value", "unit", "scenes", "particles", "steps", "ms_per_step",
                                      "plain_sequential", "speedup_vs_plain", "gpu_launches", "status", "workload")}
         batched["autotune"] = {k: b["autotune"][k] for k in ("streams", "n_candidates", "sm_share_small",
-                                                              "sm_share_medium", "sm_share_large", "graph_nodes")}
+                                                              "sm_share_medium", "sm_share_large", "graph_nodes",
+                                                              "kernel_nodes", "table_scenes")}
     served = sustainable = None
     if rank == 0 and world == 1 and not args.no_served:
         served = run_served(pkg, local_rank, duration_s=20.0)

@@ -586,13 +586,37 @@ struct Scene : SceneBase {
         if (c != 0 && c != 1) return GMPM_INVALID_ARG;
         return launch_one(s, c, nullptr, false);
     }
-    void commit_substeps(int nsub) override {
-        launches += (int64_t)nsub * kernels_per_substep();  // as launched by a captured substep
+    void commit_substeps(int nsub, bool own_launches = true) override {
+        if (own_launches) launches += (int64_t)nsub * kernels_per_substep();  // as launched by a captured substep
         if (nsub & 1) cur = 1 - cur;
         binned = false;
     }
     void set_sm_share(int sms) override { share_ = sms > 0 ? sms : 0; }
     int sm_share() const override { return share_; }
+    int batch_kind() const override {
+        if (implicit_pf()) return -1;
+        const LaunchCfg lc = cfg();
+        return (sizeof(R) == 8 ? 8 : 0) | (desc.deterministic ? 4 : 0) | (lc.other_models ? 2 : 0) |
+               (desc.precision == GMPM_PRECISION_FP32_FP64SVD ? 1 : 0);
+    }
+    void batch_args(int c, void* out) const override {
+        SceneArgs<R>& a = *static_cast<SceneArgs<R>*>(out);
+        a.sc = d_sc;
+        a.sc64 = d_sc64;
+        a.in = st[c];
+        a.out = st[1 - c];
+        a.aux = aux;
+        a.bin = bin;
+        a.grid = grid;
+        a.cnt = d_cnt;
+        a.scan = scan;
+    }
+    void batch_sizes(int64_t* n_out, uint32_t* key_space, int* nb_cap, int* ng_cap) const override {
+        *n_out = n;
+        *key_space = bin.key_space;
+        *nb_cap = bin.nb_cap;
+        *ng_cap = bin.ng_cap;
+    }
 
     // ---- checkpoint ---------------------------------------------------------
     // Every particle plane of the current state, in the internal order, with

@@ -1,25 +1,35 @@
-// Batched stepping of independent scenes: one CUDA graph per substep holds
-// every scene's binning, P2G, grid update and G2P as parallel branches, so a
-// batch of uneven scenes (each with its own SPGrid) is advanced by one graph
-// launch instead of one launch sequence per scene (the reference steps one
-// scene per MPMSimulator::simulateStick call, Simulator.cpp:227-259).
+// Batched stepping of independent scenes (the reference steps one scene per
+// MPMSimulator::simulateStick call, Simulator.cpp:227-259).  A batch of
+// uneven scenes, each with its own SPGrid, advances by one CUDA graph launch
+// per substep.
+//
+// Scene table: the scenes whose kernels are of one kind (precision, P2G mode,
+// energy models, FP64 fallback) form a group, and the group's substep is one
+// launch per stage over all its scenes (launch_batch_*, kernels.h): a device
+// array of the scenes' buffers and, per stage, each scene's range of CTAs.
+// A graph therefore holds the same 25 kernel nodes per group whatever the
+// number of scenes, and small scenes' stages fill the device together.
+// Scenes that cannot join a group (the implicit phase field, whose solve
+// stops on a device flag) are captured as their own launch sequences on
+// parallel branches.
 //
 // The substep flips each scene's double-buffered particle state, so a batch
 // keeps two graphs: graph k steps scene i from buffer parity0[i] ^ k, and
 // replays alternate between them.  A scene stepped outside the batch changes
 // its parity; the batch notices and captures again.
 //
-// Autotuner: launch shapes are sized per scene for a share of the SMs
-// (small shares let small scenes' kernels run side by side).  The tuner
-// times candidate shares per scene size class, and the number of concurrent
-// branches, on the first substeps (real substeps: results do not depend on
-// launch shapes) and keeps the fastest.
+// Autotuner: the per-scene CTA ranges of the page- and slot-parallel stages
+// (canon, P2G, grid, G2P) are sized for a share of the SMs per scene size
+// class; the tuner times candidate shares (and, for branch scenes, the
+// number of concurrent branches) on the first substeps (real substeps:
+// results do not depend on launch shapes) and keeps the fastest.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <new>
 #include <vector>
 
+#include "kernels.h"
 #include "scene.h"
 
 namespace gmpm {
@@ -43,8 +53,23 @@ struct Candidate {
 
 }  // namespace
 
+// Scenes of one kernel kind advanced by one launch per stage.
+struct Group {
+    int kind = 0;                      // SceneBase::batch_kind
+    std::vector<int> members;          // indices into Batch::sc
+    void* d_args[2] = {nullptr, nullptr};  // SceneArgs<R>[members] for graph k = 0, 1
+    int32_t* d_start = nullptr;        // kBatchMaps x (members + 1) CTA range starts
+    BatchPlan plan{};
+    bool fp64() const { return (kind & 8) != 0; }
+    size_t args_bytes() const {
+        return members.size() * (fp64() ? sizeof(SceneArgs<double>) : sizeof(SceneArgs<float>));
+    }
+};
+
 struct Batch {
     gmpm_context* ctx = nullptr;
+    std::vector<Group> groups;
+    std::vector<int> branch;           // scenes captured as their own launch sequences
     std::vector<SceneBase*> sc;
     std::vector<uint64_t> uids;
     std::vector<int> parity0;
@@ -54,6 +79,8 @@ struct Batch {
     std::vector<cudaEvent_t> join;
     cudaEvent_t fork = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaEvent_t last = nullptr;  // after the latest graph launch
+    bool launched = false;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int streams = 1;
     Candidate current{};
@@ -62,7 +89,7 @@ struct Batch {
     bool tuned = false;
     double best_ms = 0;
     Candidate best{};
-    int64_t captures = 0, substeps = 0, graph_nodes = 0;
+    int64_t captures = 0, substeps = 0, graph_nodes = 0, kernel_nodes = 0;
     double capture_s = 0;
 
     ~Batch() { release(); }
@@ -76,6 +103,18 @@ struct Batch {
     }
     void release() {
         release_graphs();
+        // The tables may still be read by launched graphs: free them in stream
+        // order after the last launch, without waiting on the host.
+        if (cap) {
+            if (launched) cudaStreamWaitEvent(cap, last, 0);
+            for (Group& g : groups) {
+                for (void*& p : g.d_args)
+                    if (p) cudaFreeAsync(p, cap), p = nullptr;
+                if (g.d_start) cudaFreeAsync(g.d_start, cap), g.d_start = nullptr;
+            }
+        }
+        if (last) cudaEventDestroy(last);
+        last = nullptr;
         for (auto s : pool) cudaStreamDestroy(s);
         for (auto e : join) cudaEventDestroy(e);
         pool.clear();
@@ -100,8 +139,33 @@ struct Batch {
             sc.push_back(s);
             uids.push_back(s->uid());
         }
+        // group the scenes by kernel kind; the rest go on branches
+        for (int i = 0; i < n; ++i) {
+            const int kind = sc[i]->batch_kind();
+            if (kind < 0) {
+                branch.push_back(i);
+                continue;
+            }
+            Group* g = nullptr;
+            for (Group& q : groups)
+                if (q.kind == kind) g = &q;
+            if (!g) {
+                groups.emplace_back();
+                g = &groups.back();
+                g->kind = kind;
+            }
+            g->members.push_back(i);
+        }
         const int max_streams = std::max(1, std::min<int>(n, 64));
         BATCH_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        BATCH_TRY(cudaEventCreateWithFlags(&last, cudaEventDisableTiming));
+        for (Group& g : groups) {
+            const size_t m = g.members.size();
+            for (void*& p : g.d_args) BATCH_TRY(cudaMallocAsync(&p, g.args_bytes(), cap));
+            BATCH_TRY(cudaMallocAsync(reinterpret_cast<void**>(&g.d_start), sizeof(int32_t) * kBatchMaps * (m + 1),
+                                      cap));
+        }
+        BATCH_TRY(cudaStreamSynchronize(cap));
         BATCH_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
         BATCH_TRY(cudaEventCreate(&t0));
         BATCH_TRY(cudaEventCreate(&t1));
@@ -135,8 +199,75 @@ struct Batch {
                 cands.push_back(c);
             }
         }
-        for (int st : {8, 16, 64})
-            if (st <= max_streams && st != default_streams) cands.push_back(Candidate{{0, 0, 0}, st});
+        if (!branch.empty())
+            for (int st : {8, 16, 64})
+                if (st <= max_streams && st != default_streams) cands.push_back(Candidate{{0, 0, 0}, st});
+    }
+
+    // Device tables of the groups for the scenes' current parities and shares
+    // (outside any capture).
+    gmpm_status prepare_tables() {
+        if (launched && !groups.empty()) BATCH_TRY(cudaEventSynchronize(last));  // no launch still reads them
+        for (Group& g : groups) {
+            const int m = (int)g.members.size();
+            std::vector<int32_t> start((size_t)kBatchMaps * (m + 1));
+            int totals[kBatchMaps] = {};
+            for (int q = 0; q < m; ++q) {
+                SceneBase* s = sc[g.members[q]];
+                int64_t np = 0;
+                uint32_t ks = 0;
+                int nb_cap = 0, ng_cap = 0;
+                s->batch_sizes(&np, &ks, &nb_cap, &ng_cap);
+                const int share = s->sm_share() > 0 ? std::min(s->sm_share(), ctx->num_sms) : ctx->num_sms;
+                int ctas[kBatchMaps];
+                batch_scene_ctas(np, ks, nb_cap, ng_cap, share, g.fp64() ? 8 : 4, ctas);
+                for (int k = 0; k < kBatchMaps; ++k) {
+                    start[(size_t)k * (m + 1) + q] = totals[k];
+                    totals[k] += ctas[k];
+                }
+            }
+            for (int k = 0; k < kBatchMaps; ++k) {
+                start[(size_t)k * (m + 1) + m] = totals[k];
+                g.plan.start[k] = g.d_start + (size_t)k * (m + 1);
+                g.plan.total[k] = totals[k];
+            }
+            g.plan.n_scenes = m;
+            g.plan.deterministic = (g.kind & 4) != 0;
+            g.plan.other_models = (g.kind & 2) != 0;
+            g.plan.fallback = (g.kind & 1) != 0;
+            // on the batch's own stream: the copies wait for nothing else on the device
+            BATCH_TRY(cudaMemcpyAsync(g.d_start, start.data(), sizeof(int32_t) * start.size(), cudaMemcpyHostToDevice,
+                                      cap));
+            const size_t one = g.fp64() ? sizeof(SceneArgs<double>) : sizeof(SceneArgs<float>);
+            std::vector<unsigned char> host(g.args_bytes());
+            for (int k = 0; k < 2; ++k) {
+                for (int q = 0; q < m; ++q) {
+                    const int i = g.members[q];
+                    sc[i]->batch_args(parity0[i] ^ k, host.data() + (size_t)q * one);
+                }
+                BATCH_TRY(cudaMemcpyAsync(g.d_args[k], host.data(), host.size(), cudaMemcpyHostToDevice, cap));
+                BATCH_TRY(cudaStreamSynchronize(cap));  // the host buffer is reused
+            }
+        }
+        return GMPM_OK;
+    }
+
+    gmpm_status launch_group(const Group& g, int k, cudaStream_t s) {
+        cudaError_t e;
+        if (g.fp64()) {
+            const auto* a = static_cast<const SceneArgs<double>*>(g.d_args[k]);
+            e = launch_batch_binning<double>(a, g.plan, s);
+            if (e == cudaSuccess) e = launch_batch_p2g<double>(a, g.plan, s);
+            if (e == cudaSuccess) e = launch_batch_grid<double>(a, g.plan, s);
+            if (e == cudaSuccess) e = launch_batch_g2p<double>(a, g.plan, s);
+        } else {
+            const auto* a = static_cast<const SceneArgs<float>*>(g.d_args[k]);
+            e = launch_batch_binning<float>(a, g.plan, s);
+            if (e == cudaSuccess) e = launch_batch_p2g<float>(a, g.plan, s);
+            if (e == cudaSuccess) e = launch_batch_grid<float>(a, g.plan, s);
+            if (e == cudaSuccess) e = launch_batch_g2p<float>(a, g.plan, s);
+        }
+        return e == cudaSuccess ? GMPM_OK : cuda_status(e);
     }
 
     void apply(const Candidate& c) {
@@ -159,9 +290,11 @@ struct Batch {
         cudaError_t e = cudaEventRecord(fork, cap);
         for (int j = 0; j < streams && e == cudaSuccess; ++j) e = cudaStreamWaitEvent(pool[j], fork, 0);
         if (e != cudaSuccess) r = cuda_status(e);
-        // largest scenes first, spread round-robin over the branches
-        std::vector<int> order(sc.size());
-        for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+        // the groups, one launch per stage each, on the capture stream
+        for (const Group& g : groups)
+            if (r == GMPM_OK) r = launch_group(g, k, cap);
+        // branch scenes: largest first, spread round-robin over the branches
+        std::vector<int> order(branch);
         std::stable_sort(order.begin(), order.end(),
                          [&](int a, int b) { return sc[a]->particles() > sc[b]->particles(); });
         for (size_t q = 0; q < order.size() && r == GMPM_OK; ++q) {
@@ -180,6 +313,14 @@ struct Batch {
             size_t nodes = 0;
             cudaGraphGetNodes(g, nullptr, &nodes);
             graph_nodes = (int64_t)nodes;
+            std::vector<cudaGraphNode_t> list(nodes);
+            kernel_nodes = 0;
+            if (nodes && cudaGraphGetNodes(g, list.data(), &nodes) == cudaSuccess)
+                for (cudaGraphNode_t nd : list) {
+                    cudaGraphNodeType type;
+                    if (cudaGraphNodeGetType(nd, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel)
+                        ++kernel_nodes;
+                }
             e = cudaGraphInstantiate(out, g, 0);
             if (e != cudaSuccess) r = cuda_status(e);
         }
@@ -201,7 +342,9 @@ struct Batch {
             release_graphs();
             parity0.resize(sc.size());
             for (size_t i = 0; i < sc.size(); ++i) parity0[i] = sc[i]->parity();
-            gmpm_status r = capture(0, &exec[0]);
+            gmpm_status r = prepare_tables();
+            if (r != GMPM_OK) return r;
+            r = capture(0, &exec[0]);
             if (r == GMPM_OK) r = capture(1, &exec[1]);
             if (r != GMPM_OK) {
                 release_graphs();
@@ -221,7 +364,10 @@ struct Batch {
             gmpm_status r = ensure_graphs(&k);
             if (r != GMPM_OK) return r;
             BATCH_TRY(cudaGraphLaunch(exec[k], s));
-            for (SceneBase* q : sc) q->commit_substeps(1);
+            BATCH_TRY(cudaEventRecord(last, s));
+            launched = true;
+            // a table scene's kernels are the group's launches, counted by the batch (kernel_nodes)
+            for (size_t i = 0; i < sc.size(); ++i) sc[i]->commit_substeps(1, sc[i]->batch_kind() < 0);
             ++substeps;
         }
         return GMPM_OK;
@@ -281,6 +427,10 @@ struct Batch {
         o->sm_share_medium = current.share[1];
         o->sm_share_large = current.share[2];
         o->capture_seconds = capture_s;
+        o->kernel_nodes = kernel_nodes;
+        int t = 0;
+        for (const Group& g : groups) t += (int)g.members.size();
+        o->table_scenes = t;
     }
 };
 

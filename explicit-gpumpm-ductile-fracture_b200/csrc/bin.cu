@@ -23,13 +23,15 @@ namespace gmpm {
 constexpr int kBinThreads = 256;
 constexpr int kBinILP = 4;
 
+// The kernels' bodies take the CTA's index within its scene's share of the
+// launch (VB, common.cuh); the __global__ wrappers below each body serve a
+// one-scene launch, the batched launches at the end of this file many scenes.
 template <typename R>
-__global__ void __launch_bounds__(kBinThreads) k_bin_keys(int64_t n, const R* __restrict__ x0,
-                                                          const R* __restrict__ x1, const R* __restrict__ x2,
-                                                          const SceneDev<R>* __restrict__ sc,
-                                                          uint32_t* __restrict__ keys,
-                                                          uint8_t* __restrict__ page_flag, Counters* cnt) {
-    const int64_t i0 = (int64_t)blockIdx.x * kBinThreads * kBinILP + threadIdx.x;
+__device__ __forceinline__ void bin_keys_body(VB vb, int64_t n, const R* __restrict__ x0, const R* __restrict__ x1,
+                                              const R* __restrict__ x2, const SceneDev<R>* __restrict__ sc,
+                                              uint32_t* __restrict__ keys, uint8_t* __restrict__ page_flag,
+                                              Counters* cnt) {
+    const int64_t i0 = (int64_t)vb.b * kBinThreads * kBinILP + threadIdx.x;
     const double inv_dx = sc->inv_dx_d;
     int hi[3];
 #pragma unroll
@@ -73,10 +75,20 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_keys(int64_t n, const R* __
     if (bad) raise_flag(cnt, GMPM_FLAG_OUT_OF_DOMAIN);
 }
 
+template <typename R>
+__global__ void __launch_bounds__(kBinThreads) k_bin_keys(int64_t n, const R* __restrict__ x0,
+                                                          const R* __restrict__ x1, const R* __restrict__ x2,
+                                                          const SceneDev<R>* __restrict__ sc,
+                                                          uint32_t* __restrict__ keys,
+                                                          uint8_t* __restrict__ page_flag, Counters* cnt) {
+    bin_keys_body<R>(own_blocks(), n, x0, x1, x2, sc, keys, page_flag, cnt);
+}
+
 // Mark every active page and its 7 "+" neighbours as grid pages
 // (supplementAdjacentPages, Transformer_kernal.cu:70-96).
-__global__ void k_mark_grid(uint32_t key_space, const uint8_t* __restrict__ page_flag, uint8_t* __restrict__ grid_flag) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void mark_grid_body(VB vb, uint32_t key_space, const uint8_t* __restrict__ page_flag,
+                                               uint8_t* __restrict__ grid_flag) {
+    const uint32_t k = vb.b * blockDim.x + threadIdx.x;
     if (k >= key_space || !page_flag[k]) return;
     int bx, by, bz;
     page_coords(k, bx, by, bz);
@@ -84,10 +96,15 @@ __global__ void k_mark_grid(uint32_t key_space, const uint8_t* __restrict__ page
     for (int d = 0; d < 8; ++d) grid_flag[page_key(bx + (d >> 2), by + ((d >> 1) & 1), bz + (d & 1))] = 1;
 }
 
+__global__ void k_mark_grid(uint32_t key_space, const uint8_t* __restrict__ page_flag, uint8_t* __restrict__ grid_flag) {
+    mark_grid_body(own_blocks(), key_space, page_flag, grid_flag);
+}
+
 // Compact flagged keys into ascending order.
-__global__ void k_compact_keys(uint32_t key_space, const uint8_t* __restrict__ flag, const int32_t* __restrict__ rank,
-                               uint32_t* __restrict__ out, int cap, Counters* cnt) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void compact_keys_body(VB vb, uint32_t key_space, const uint8_t* __restrict__ flag,
+                                                  const int32_t* __restrict__ rank, uint32_t* __restrict__ out,
+                                                  int cap, Counters* cnt) {
+    const uint32_t k = vb.b * blockDim.x + threadIdx.x;
     if (k >= key_space || !flag[k]) return;
     const int r = rank[k];
     if (r < cap)
@@ -96,12 +113,17 @@ __global__ void k_compact_keys(uint32_t key_space, const uint8_t* __restrict__ f
         raise_flag(cnt, GMPM_FLAG_TABLE_OVERFLOW);
 }
 
+__global__ void k_compact_keys(uint32_t key_space, const uint8_t* __restrict__ flag, const int32_t* __restrict__ rank,
+                               uint32_t* __restrict__ out, int cap, Counters* cnt) {
+    compact_keys_body(own_blocks(), key_space, flag, rank, out, cap, cnt);
+}
+
 // Page topology: adj (establishPageTopology, Transformer_kernal.cu:98-114) and
 // its inverse grid_src used by the fixed-order grid gather.
-__global__ void k_page_links(BinDev bin, const Counters* cnt) {
+__device__ __forceinline__ void page_links_body(VB vb, const BinDev& bin, const Counters* cnt) {
     const int nb = min(cnt->n_blocks, bin.nb_cap);
     const int ng = min(cnt->n_grid_blocks, bin.ng_cap);
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = vb.b * blockDim.x + threadIdx.x;
     const int slot = t & 7;
     const int idx = t >> 3;
     const int di = slot >> 2, dj = (slot >> 1) & 1, dk = slot & 1;
@@ -126,11 +148,13 @@ __global__ void k_page_links(BinDev bin, const Counters* cnt) {
     }
 }
 
+__global__ void k_page_links(BinDev bin, const Counters* cnt) { page_links_body(own_blocks(), bin, cnt); }
+
 // Histogram of (page rank, cell) buckets with warp-aggregated atomics.
-__global__ void __launch_bounds__(kBinThreads) k_bin_hist(int64_t n, const uint32_t* __restrict__ keys,
-                                                          const int32_t* __restrict__ page_rank,
-                                                          int32_t* __restrict__ cell_count, int nb_cap) {
-    const int64_t i0 = (int64_t)blockIdx.x * kBinThreads * kBinILP + threadIdx.x;
+__device__ __forceinline__ void bin_hist_body(VB vb, int64_t n, const uint32_t* __restrict__ keys,
+                                              const int32_t* __restrict__ page_rank, int32_t* __restrict__ cell_count,
+                                              int nb_cap) {
+    const int64_t i0 = (int64_t)vb.b * kBinThreads * kBinILP + threadIdx.x;
     uint32_t key[kBinILP];
     int rank[kBinILP];
 #pragma unroll
@@ -147,13 +171,19 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_hist(int64_t n, const uint3
     }
 }
 
+__global__ void __launch_bounds__(kBinThreads) k_bin_hist(int64_t n, const uint32_t* __restrict__ keys,
+                                                          const int32_t* __restrict__ page_rank,
+                                                          int32_t* __restrict__ cell_count, int nb_cap) {
+    bin_hist_body(own_blocks(), n, keys, page_rank, cell_count, nb_cap);
+}
+
 // Scatter slots; lanes of one warp with the same bucket keep their order.
-__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys,
-                                                             const int32_t* __restrict__ page_rank,
-                                                             const int32_t* __restrict__ cell_start,
-                                                             int32_t* __restrict__ fill, int32_t* __restrict__ perm,
-                                                             uint32_t* __restrict__ keys_sorted, int nb_cap) {
-    const int64_t i0 = (int64_t)blockIdx.x * kBinThreads * kBinILP + threadIdx.x;
+__device__ __forceinline__ void bin_scatter_body(VB vb, int64_t n, const uint32_t* __restrict__ keys,
+                                                 const int32_t* __restrict__ page_rank,
+                                                 const int32_t* __restrict__ cell_start, int32_t* __restrict__ fill,
+                                                 int32_t* __restrict__ perm, uint32_t* __restrict__ keys_sorted,
+                                                 int nb_cap) {
+    const int64_t i0 = (int64_t)vb.b * kBinThreads * kBinILP + threadIdx.x;
     uint32_t key[kBinILP];
     int bucket[kBinILP], start[kBinILP];
 #pragma unroll
@@ -179,6 +209,14 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(int64_t n, const ui
             keys_sorted[slot] = key[u];
         }
     }
+}
+
+__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(int64_t n, const uint32_t* __restrict__ keys,
+                                                             const int32_t* __restrict__ page_rank,
+                                                             const int32_t* __restrict__ cell_start,
+                                                             int32_t* __restrict__ fill, int32_t* __restrict__ perm,
+                                                             uint32_t* __restrict__ keys_sorted, int nb_cap) {
+    bin_scatter_body(own_blocks(), n, keys, page_rank, cell_start, fill, perm, keys_sorted, nb_cap);
 }
 
 // Canonical in-cell order: ascending previous slot.  Each warp takes one page
@@ -231,7 +269,7 @@ __device__ __forceinline__ void canon_rank_warp(const BinDev& bin, const int32_t
     }
 }
 
-__global__ void __launch_bounds__(32 * kCanonWarps) k_bin_canon(BinDev bin, Counters* cnt) {
+__device__ __forceinline__ void bin_canon_body(VB vb, const BinDev& bin, Counters* cnt) {
     __shared__ int32_t buf[kCanonBuf];
     __shared__ int32_t cs[kCanonWarps][68];
     __shared__ uint8_t bad[kCanonWarps][64];
@@ -239,7 +277,7 @@ __global__ void __launch_bounds__(32 * kCanonWarps) k_bin_canon(BinDev bin, Coun
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nb = min(cnt->n_blocks, bin.nb_cap);
     int32_t* wbuf = buf + warp * kCanonWarpBuf;
-    for (int g = blockIdx.x * kCanonWarps; g < nb; g += gridDim.x * kCanonWarps) {
+    for (int g = vb.b * kCanonWarps; g < nb; g += vb.g * kCanonWarps) {
         const int b = g + warp;
         int is_big = 0;
         if (b < nb) {
@@ -279,6 +317,10 @@ __global__ void __launch_bounds__(32 * kCanonWarps) k_bin_canon(BinDev bin, Coun
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(32 * kCanonWarps) k_bin_canon(BinDev bin, Counters* cnt) {
+    bin_canon_body(own_blocks(), bin, cnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -333,7 +375,6 @@ cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bi
 
 template <typename R>
 cudaError_t launch_keys(const SceneDev<R>* sc, const PState<R>& st, BinDev bin, Counters* cnt, cudaStream_t s) {
-    const int T = 256;
     k_bin_keys<R><<<bin_grid(bin.n), kBinThreads, 0, s>>>(bin.n, st.x[0], st.x[1], st.x[2], sc, bin.keys,
                                                                  bin.page_flag, cnt);
     return cudaGetLastError();
@@ -348,6 +389,196 @@ cudaError_t launch_mark_grid(BinDev bin, cudaStream_t s) {
     k_mark_grid<<<(bin.key_space + T - 1) / T, T, 0, s>>>(bin.key_space, bin.page_flag, bin.grid_flag);
     return cudaGetLastError();
 }
+
+// ---- batched binning over many scenes ------------------------------------------
+
+void batch_scene_ctas(int64_t n, uint32_t key_space, int nb_cap, int ng_cap, int sms, int real_bytes,
+                      int ctas[kBatchMaps]) {
+    auto cdiv = [](int64_t a, int64_t b) { return (int)std::max<int64_t>(1, (a + b - 1) / b); };
+    const int64_t ncell = (int64_t)nb_cap * 64;
+    ctas[BM_ZERO_FLAGS] = cdiv(key_space, 4096);
+    ctas[BM_PARTICLES] = (int)bin_grid(n);
+    ctas[BM_KEYSPACE] = cdiv(key_space, 256);
+    ctas[BM_KEY_TILES] = cdiv(key_space, kScanTile);
+    ctas[BM_LINKS] = cdiv((int64_t)std::max(nb_cap, ng_cap) * 8, 256);
+    ctas[BM_ZERO_CELLS] = cdiv(ncell * 4, 4096);
+    ctas[BM_CELL_TILES] = cdiv(ncell, kScanTile);
+    ctas[BM_CANON] = std::max(1, std::min(cdiv(nb_cap, kCanonWarps), sms * 8));
+    ctas[BM_P2G] = std::max(1, std::min(nb_cap, sms));
+    ctas[BM_GRID] = std::max(1, std::min(ng_cap / 4 + 1, sms * 8));
+    const int per_sm = real_bytes == 4 ? 2 : 1;  // G2P's resident CTAs per SM
+    ctas[BM_G2P] = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * per_sm));
+    ctas[BM_ONE] = 1;
+}
+
+// Zero `bytes` (a multiple of 4) from p: 4 KiB per CTA.
+__device__ __forceinline__ void zero_bytes_body(VB vb, void* p, int64_t bytes) {
+    char* c = static_cast<char*>(p);
+    const int64_t off = (int64_t)vb.b * 4096 + (int64_t)threadIdx.x * 16;
+    if (off + 16 <= bytes && ((reinterpret_cast<uintptr_t>(c) & 15) == 0)) {
+        *reinterpret_cast<uint4*>(c + off) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+        for (int q = 0; q < 16; q += 4)
+            if (off + q + 4 <= bytes) *reinterpret_cast<uint32_t*>(c + off + q) = 0u;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_batch_zero(const SceneArgs<R>* __restrict__ A, const int32_t* __restrict__ start,
+                                                    int ns, int which) {
+    VB vb;
+    const BinDev& bin = A[scene_of_block(start, ns, vb)].bin;
+    if (which == 0) zero_bytes_body(vb, bin.page_flag, bin.key_space);
+    if (which == 1) zero_bytes_body(vb, bin.grid_flag, bin.key_space);
+    if (which == 2) zero_bytes_body(vb, bin.cell_count, (int64_t)bin.nb_cap * 64 * 4);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBinThreads) k_batch_keys(const SceneArgs<R>* __restrict__ A,
+                                                            const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    bin_keys_body<R>(vb, a.bin.n, a.in.x[0], a.in.x[1], a.in.x[2], a.sc, a.bin.keys, a.bin.page_flag, a.cnt);
+}
+
+// The three scans of the binning: 0 page flags -> page ranks, 1 grid flags ->
+// grid ranks, 2 cell counts -> cell starts.
+template <int kWhich>
+struct ScanSel;
+template <>
+struct ScanSel<0> {
+    using T = uint8_t;
+    static __device__ const T* in(const BinDev& b) { return b.page_flag; }
+    static __device__ int64_t n(const BinDev& b) { return b.key_space; }
+    static __device__ int32_t* out(const BinDev& b) { return b.page_rank; }
+    static __device__ int32_t* total(const BinDev& b, Counters* c) { return &c->n_blocks; }
+};
+template <>
+struct ScanSel<1> {
+    using T = uint8_t;
+    static __device__ const T* in(const BinDev& b) { return b.grid_flag; }
+    static __device__ int64_t n(const BinDev& b) { return b.key_space; }
+    static __device__ int32_t* out(const BinDev& b) { return b.grid_rank; }
+    static __device__ int32_t* total(const BinDev& b, Counters* c) { return &c->n_grid_blocks; }
+};
+template <>
+struct ScanSel<2> {
+    using T = int32_t;
+    static __device__ const T* in(const BinDev& b) { return b.cell_count; }
+    static __device__ int64_t n(const BinDev& b) { return (int64_t)b.nb_cap * 64; }
+    static __device__ int32_t* out(const BinDev& b) { return b.cell_start; }
+    static __device__ int32_t* total(const BinDev& b, Counters*) { return b.cell_start + (int64_t)b.nb_cap * 64; }
+};
+
+template <typename R, int kWhich>
+__global__ void __launch_bounds__(kScanThreads) k_batch_scan_reduce(const SceneArgs<R>* __restrict__ A,
+                                                                    const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    using S = ScanSel<kWhich>;
+    scan_reduce_body(vb, S::in(a.bin), S::n(a.bin), a.scan.tile_sums);
+}
+
+template <typename R, int kWhich>
+__global__ void __launch_bounds__(kScanThreads) k_batch_scan_tiles(const SceneArgs<R>* __restrict__ A,
+                                                                   const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    using S = ScanSel<kWhich>;
+    const int64_t ntiles = (S::n(a.bin) + kScanTile - 1) / kScanTile;
+    scan_tiles_body(a.scan.tile_sums, ntiles, S::total(a.bin, a.cnt));
+}
+
+template <typename R, int kWhich>
+__global__ void __launch_bounds__(kScanThreads) k_batch_scan_apply(const SceneArgs<R>* __restrict__ A,
+                                                                   const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    using S = ScanSel<kWhich>;
+    scan_apply_body(vb, S::in(a.bin), S::n(a.bin), a.scan.tile_sums, S::out(a.bin));
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_batch_mark(const SceneArgs<R>* __restrict__ A,
+                                                    const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const BinDev& bin = A[scene_of_block(start, ns, vb)].bin;
+    mark_grid_body(vb, bin.key_space, bin.page_flag, bin.grid_flag);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_batch_compact(const SceneArgs<R>* __restrict__ A,
+                                                       const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    compact_keys_body(vb, a.bin.key_space, a.bin.page_flag, a.bin.page_rank, a.bin.block_keys, a.bin.nb_cap, a.cnt);
+    compact_keys_body(vb, a.bin.key_space, a.bin.grid_flag, a.bin.grid_rank, a.bin.grid_keys, a.bin.ng_cap, a.cnt);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_batch_links(const SceneArgs<R>* __restrict__ A,
+                                                     const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    page_links_body(vb, a.bin, a.cnt);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBinThreads) k_batch_hist(const SceneArgs<R>* __restrict__ A,
+                                                            const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const BinDev& bin = A[scene_of_block(start, ns, vb)].bin;
+    bin_hist_body(vb, bin.n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBinThreads) k_batch_scatter(const SceneArgs<R>* __restrict__ A,
+                                                               const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const BinDev& bin = A[scene_of_block(start, ns, vb)].bin;
+    bin_scatter_body(vb, bin.n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, bin.perm, bin.keys_sorted,
+                     bin.nb_cap);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(32 * kCanonWarps) k_batch_canon(const SceneArgs<R>* __restrict__ A,
+                                                                  const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    bin_canon_body(vb, a.bin, a.cnt);
+}
+
+// The binning of every scene of a batch: the same steps as launch_binning,
+// each one launch over all scenes.
+template <typename R>
+cudaError_t launch_batch_binning(const SceneArgs<R>* A, const BatchPlan& P, cudaStream_t s) {
+    const int ns = P.n_scenes;
+    auto T = [&](int m) { return dim3((unsigned)P.total[m]); };
+    auto S = [&](int m) { return P.start[m]; };
+    cudaError_t e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_FLAGS), dim3(256), 0, s, A, S(BM_ZERO_FLAGS), ns, 0);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_FLAGS), dim3(256), 0, s, A, S(BM_ZERO_FLAGS), ns, 1);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_keys<R>, T(BM_PARTICLES), dim3(kBinThreads), 0, s, A, S(BM_PARTICLES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_reduce<R, 0>, T(BM_KEY_TILES), dim3(kScanThreads), 0, s, A, S(BM_KEY_TILES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_tiles<R, 0>, T(BM_ONE), dim3(kScanThreads), 0, s, A, S(BM_ONE), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_apply<R, 0>, T(BM_KEY_TILES), dim3(kScanThreads), 0, s, A, S(BM_KEY_TILES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_mark<R>, T(BM_KEYSPACE), dim3(256), 0, s, A, S(BM_KEYSPACE), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_reduce<R, 1>, T(BM_KEY_TILES), dim3(kScanThreads), 0, s, A, S(BM_KEY_TILES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_tiles<R, 1>, T(BM_ONE), dim3(kScanThreads), 0, s, A, S(BM_ONE), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_apply<R, 1>, T(BM_KEY_TILES), dim3(kScanThreads), 0, s, A, S(BM_KEY_TILES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_compact<R>, T(BM_KEYSPACE), dim3(256), 0, s, A, S(BM_KEYSPACE), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_links<R>, T(BM_LINKS), dim3(256), 0, s, A, S(BM_LINKS), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_CELLS), dim3(256), 0, s, A, S(BM_ZERO_CELLS), ns, 2);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_hist<R>, T(BM_PARTICLES), dim3(kBinThreads), 0, s, A, S(BM_PARTICLES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_reduce<R, 2>, T(BM_CELL_TILES), dim3(kScanThreads), 0, s, A, S(BM_CELL_TILES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_tiles<R, 2>, T(BM_ONE), dim3(kScanThreads), 0, s, A, S(BM_ONE), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scan_apply<R, 2>, T(BM_CELL_TILES), dim3(kScanThreads), 0, s, A, S(BM_CELL_TILES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_CELLS), dim3(256), 0, s, A, S(BM_ZERO_CELLS), ns, 2);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_scatter<R>, T(BM_PARTICLES), dim3(kBinThreads), 0, s, A, S(BM_PARTICLES), ns);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_canon<R>, T(BM_CANON), dim3(32 * kCanonWarps), 0, s, A, S(BM_CANON), ns);
+    return e;
+}
+template cudaError_t launch_batch_binning<float>(const SceneArgs<float>*, const BatchPlan&, cudaStream_t);
+template cudaError_t launch_batch_binning<double>(const SceneArgs<double>*, const BatchPlan&, cudaStream_t);
 
 template cudaError_t launch_binning<float>(const SceneDev<float>*, const PState<float>&, BinDev, ScanScratch,
                                            Counters*, int, cudaStream_t);

@@ -132,4 +132,32 @@ __host__ __device__ inline void page_coords(uint32_t key, int& bx, int& by, int&
 
 __device__ inline void raise_flag(Counters* c, unsigned int f) { atomicOr(&c->flags, f); }
 
+// ---- launches over one scene or many ------------------------------------------
+// A kernel body sees its CTA's index and the CTA count of its scene's share of
+// the launch: the CUDA block index and grid size in a one-scene launch, or the
+// CTA's place in its scene's range in a batched launch over many scenes.
+struct VB {
+    int b, g;
+};
+__device__ __forceinline__ VB own_blocks() { return VB{(int)blockIdx.x, (int)gridDim.x}; }
+
+// Batched launch: scene s owns CTAs [start[s], start[s + 1]) (n_scenes + 1
+// entries, every scene at least one CTA).  Returns the scene of this CTA and
+// its place in the scene's range.
+__device__ __forceinline__ int scene_of_block(const int32_t* __restrict__ start, int n_scenes, VB& v) {
+    const int b = (int)blockIdx.x;
+    int lo = 0, hi = n_scenes - 1;  // the last scene whose range starts at or before b
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&start[mid]) <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int s0 = __ldg(&start[lo]);
+    v.b = b - s0;
+    v.g = __ldg(&start[lo + 1]) - s0;
+    return lo;
+}
+
 }  // namespace gmpm

@@ -18,6 +18,7 @@
 #include "async_copy.cuh"
 #include "constitutive.cuh"
 #include "kernels.h"
+#include "launch.cuh"
 
 namespace gmpm {
 
@@ -270,7 +271,8 @@ __device__ __forceinline__ void gather_stencil<float>(const float (*__restrict__
 }
 
 // Unit sequence of one CTA: slots [b T / C, (b + 1) T / C) of the T sorted
-// slots, C = gridDim.x, in units of up to kG2PUnit slots and kUnitPages pages.
+// slots, b the CTA's index and C the CTA count of its scene's share of the
+// launch, in units of up to kG2PUnit slots and kUnitPages pages.
 // Every thread runs the same iterator in step (it shuffles), so it is called
 // by all threads of the CTA at the same points.  Page starts cs(q) =
 // cell_start[64 q] are held 32 pages at a time in lane registers, the next
@@ -285,11 +287,11 @@ struct UnitIter {
         q = min(q, nb);
         return bin.cell_start[(int64_t)q * 64];
     }
-    __device__ void init(const BinDev& bin, int nb_) {
+    __device__ void init(const BinDev& bin, int nb_, VB vb) {
         nb = nb_;
         total = nb > 0 ? bin.cell_start[(int64_t)nb * 64] : 0;
-        s = (int64_t)blockIdx.x * total / gridDim.x;
-        se = (int64_t)(blockIdx.x + 1) * total / gridDim.x;
+        s = (int64_t)vb.b * total / vb.g;
+        se = (int64_t)(vb.b + 1) * total / vb.g;
         p = 0;
         if (s < se) p = bin.page_rank[bin.keys_sorted[s] >> 6];
         seq = 0;
@@ -390,9 +392,10 @@ __device__ __forceinline__ void issue_data(G2PShared<R>& S, int m, int buf, int 
 // kernel spill (76-136 bytes at 128 registers), so scenes without it launch
 // the instantiation that leaves it out (126 registers, no spills).
 template <typename R, bool kAnyModel, bool kFallback>
-__global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
-    k_g2p(const SceneDev<R>* __restrict__ sc, const SceneDev<double>* __restrict__ sc64, PState<R> in,
-          PState<R> out, PAux<R> aux, BinDev bin, const R* __restrict__ nodes, Counters* cnt) {
+__device__ __forceinline__ void g2p_body(VB vb, const SceneDev<R>* __restrict__ sc,
+                                         const SceneDev<double>* __restrict__ sc64, const PState<R>& in,
+                                         const PState<R>& out, const PAux<R>& aux, const BinDev& bin,
+                                         const R* __restrict__ nodes, Counters* cnt) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     G2PShared<R>& S = *reinterpret_cast<G2PShared<R>*>(smem_raw);
     const int t = threadIdx.x;
@@ -405,7 +408,7 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
 
     // prologue: meta of units 0 and 1, data of unit 0
     UnitIter it;
-    it.init(bin, nb);
+    it.init(bin, nb, vb);
     int d0[7], d1[7];  // s0, n, seq0, np, c1, c2, p0
     it.step(bin, d0[0], d0[1], d0[2], d0[3], d0[4], d0[5], d0[6]);
     it.step(bin, d1[0], d1[1], d1[2], d1[3], d1[4], d1[5], d1[6]);
@@ -574,8 +577,15 @@ __global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
 // in adaptive mode, set the next substep's dt from the maximum particle speed
 // of this G2P: dt = min(dt_max, cfl dx / v_max) (MPMSimulator::computeDt,
 // Simulator.cpp:200-225, on the device instead of through a host read).
+template <typename R, bool kAnyModel, bool kFallback>
+__global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
+    k_g2p(const SceneDev<R>* __restrict__ sc, const SceneDev<double>* __restrict__ sc64, PState<R> in,
+          PState<R> out, PAux<R> aux, BinDev bin, const R* __restrict__ nodes, Counters* cnt) {
+    g2p_body<R, kAnyModel, kFallback>(own_blocks(), sc, sc64, in, out, aux, bin, nodes, cnt);
+}
+
 template <typename R>
-__global__ void k_advance_time(Counters* cnt, SceneDev<R>* sc, SceneDev<double>* sc64) {
+__device__ __forceinline__ void advance_time_body(Counters* cnt, SceneDev<R>* sc, SceneDev<double>* sc64) {
     cnt->time += sc64->dt;
     cnt->substeps += 1;
     if (sc64->adaptive_dt) {
@@ -589,19 +599,66 @@ __global__ void k_advance_time(Counters* cnt, SceneDev<R>* sc, SceneDev<double>*
 }
 
 template <typename R>
+__global__ void k_advance_time(Counters* cnt, SceneDev<R>* sc, SceneDev<double>* sc64) {
+    advance_time_body<R>(cnt, sc, sc64);
+}
+
+// Batched launches: the same bodies for the scene that owns this CTA.  The
+// FP64 fallback reads the scene's FP64 block only in the form with it.
+template <typename R, bool kAnyModel, bool kFallback>
+__global__ void __launch_bounds__(kG2PUnit, sizeof(R) == 4 ? kG2PMinBlocks : 1)
+    k_batch_g2p(const SceneArgs<R>* __restrict__ A, const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    g2p_body<R, kAnyModel, kFallback>(vb, a.sc, kFallback ? a.sc64 : nullptr, a.in, a.out, a.aux, a.bin,
+                                      reinterpret_cast<const R*>(a.grid.nodes), a.cnt);
+}
+
+template <typename R>
+__global__ void k_batch_clock(const SceneArgs<R>* __restrict__ A, const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    if (threadIdx.x == 0)
+        advance_time_body<R>(a.cnt, const_cast<SceneDev<R>*>(a.sc), const_cast<SceneDev<double>*>(a.sc64));
+}
+
+template <typename R>
 cudaError_t prepare_g2p() {
     const int smem = (int)sizeof(G2PShared<R>);
-    cudaError_t e = cudaFuncSetAttribute(k_g2p<R, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_g2p<R, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e = cudaFuncSetAttribute(k_g2p<R, false, false>, attr, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_g2p<R, true, false>, attr, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch_g2p<R, false, false>, attr, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch_g2p<R, true, false>, attr, smem);
     if constexpr (sizeof(R) == 4) {
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_g2p<R, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_g2p<R, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_g2p<R, false, true>, attr, smem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_g2p<R, true, true>, attr, smem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch_g2p<R, false, true>, attr, smem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_batch_g2p<R, true, true>, attr, smem);
     }
     return e;
 }
+
+template <typename R>
+cudaError_t launch_batch_g2p(const SceneArgs<R>* A, const BatchPlan& P, cudaStream_t s) {
+    const dim3 grid((unsigned)P.total[BM_G2P]), block(kG2PUnit);
+    const size_t smem = sizeof(G2PShared<R>);
+    const int ns = P.n_scenes;
+    const int32_t* st = P.start[BM_G2P];
+    cudaError_t e;
+    const bool fb = sizeof(R) == 4 && P.fallback;
+    if (P.other_models)
+        e = fb ? launch_kernel(k_batch_g2p<R, true, (sizeof(R) == 4)>, grid, block, smem, s, A, st, ns)
+               : launch_kernel(k_batch_g2p<R, true, false>, grid, block, smem, s, A, st, ns);
+    else
+        e = fb ? launch_kernel(k_batch_g2p<R, false, (sizeof(R) == 4)>, grid, block, smem, s, A, st, ns)
+               : launch_kernel(k_batch_g2p<R, false, false>, grid, block, smem, s, A, st, ns);
+    if (e == cudaSuccess)
+        e = launch_kernel(k_batch_clock<R>, dim3((unsigned)P.total[BM_ONE]), dim3(32), 0, s, A, P.start[BM_ONE], ns);
+    return e;
+}
+template cudaError_t launch_batch_g2p<float>(const SceneArgs<float>*, const BatchPlan&, cudaStream_t);
+template cudaError_t launch_batch_g2p<double>(const SceneArgs<double>*, const BatchPlan&, cudaStream_t);
 template cudaError_t prepare_g2p<float>();
 template cudaError_t prepare_g2p<double>();
 

@@ -15,15 +15,16 @@
 #include <cstdint>
 
 #include "kernels.h"
+#include "launch.cuh"
 
 namespace gmpm {
 
 constexpr int kGridThreads = 256;  // 4 grid pages per CTA
 
 template <typename R>
-__global__ void __launch_bounds__(kGridThreads)
-    k_grid(const SceneDev<R>* __restrict__ sc, BinDev bin, const R* __restrict__ tile, R* __restrict__ nodes,
-           double* __restrict__ diag, PcgDev pcg, Counters* cnt) {
+__device__ __forceinline__ void grid_body(VB vb, const SceneDev<R>* __restrict__ sc, const BinDev& bin,
+                                          const R* __restrict__ tile, R* __restrict__ nodes,
+                                          double* __restrict__ diag, const PcgDev& pcg, Counters* cnt) {
     const int ng = min(cnt->n_grid_blocks, bin.ng_cap);
     const int node = threadIdx.x & 63;
     const int ci = node >> 4, cj = (node >> 2) & 3, ck = node & 3;
@@ -31,7 +32,7 @@ __global__ void __launch_bounds__(kGridThreads)
     const R Mob = sc->mobility;
     const double t_now = cnt->time;
     double dm = 0, dp0 = 0, dp1 = 0, dp2 = 0;
-    for (int g = blockIdx.x * 4 + (threadIdx.x >> 6); g < ng; g += gridDim.x * 4) {
+    for (int g = vb.b * 4 + (threadIdx.x >> 6); g < ng; g += vb.g * 4) {
         // fixed-order, compensated sum of the page tiles overlapping the node
         R ch[kP2GChannels], comp[kP2GChannels];
 #pragma unroll
@@ -146,6 +147,42 @@ __global__ void __launch_bounds__(kGridThreads)
         atomicAdd(&diag[3], dp2);
     }
 }
+
+template <typename R>
+__global__ void __launch_bounds__(kGridThreads)
+    k_grid(const SceneDev<R>* __restrict__ sc, BinDev bin, const R* __restrict__ tile, R* __restrict__ nodes,
+           double* __restrict__ diag, PcgDev pcg, Counters* cnt) {
+    grid_body<R>(own_blocks(), sc, bin, tile, nodes, diag, pcg, cnt);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kGridThreads)
+    k_batch_grid(const SceneArgs<R>* __restrict__ A, const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    grid_body<R>(vb, a.sc, a.bin, reinterpret_cast<const R*>(a.grid.tile), reinterpret_cast<R*>(a.grid.nodes),
+                 a.grid.diag, a.grid.pcg, a.cnt);
+}
+
+// One CTA per scene: clear the grid diagnostics the grid stage accumulates.
+template <typename R>
+__global__ void k_batch_zero_diag(const SceneArgs<R>* __restrict__ A, const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    if (threadIdx.x < 4) a.grid.diag[threadIdx.x] = 0.0;
+}
+
+template <typename R>
+cudaError_t launch_batch_grid(const SceneArgs<R>* A, const BatchPlan& P, cudaStream_t s) {
+    cudaError_t e = launch_kernel(k_batch_zero_diag<R>, dim3((unsigned)P.total[BM_ONE]), dim3(32), 0, s, A,
+                                  P.start[BM_ONE], P.n_scenes);
+    if (e == cudaSuccess)
+        e = launch_kernel(k_batch_grid<R>, dim3((unsigned)P.total[BM_GRID]), dim3(kGridThreads), 0, s, A,
+                          P.start[BM_GRID], P.n_scenes);
+    return e;
+}
+template cudaError_t launch_batch_grid<float>(const SceneArgs<float>*, const BatchPlan&, cudaStream_t);
+template cudaError_t launch_batch_grid<double>(const SceneArgs<double>*, const BatchPlan&, cudaStream_t);
 
 template <typename R>
 cudaError_t launch_grid(const SceneDev<R>* sc, BinDev bin, GridDev grid, Counters* cnt, LaunchCfg cfg,

@@ -119,4 +119,66 @@ template <typename R>
 cudaError_t launch_pack_field(const PState<R>& st, const PAux<R>& aux, int field, int dtype, int order, int64_t n,
                               void* out, cudaStream_t stream);
 
+// ---- batched launches: one launch per stage over many scenes ------------------
+// A batch of scenes of one kind (precision, P2G mode, energy models, FP64
+// fallback) advances with one launch per stage of the substep.  Every stage
+// splits its launch into per-scene CTA ranges (BatchPlan); a CTA finds its
+// scene by a search over its stage's range starts and runs the stage's body
+// for that scene with its place in the scene's range (VB, common.cuh).
+
+// One scene's buffers as the stages of a batched substep see them, for the
+// parity that reads state `in` and writes `out`.
+template <typename R>
+struct SceneArgs {
+    const SceneDev<R>* sc;
+    const SceneDev<double>* sc64;
+    PState<R> in, out;
+    PAux<R> aux;
+    BinDev bin;
+    GridDev grid;
+    Counters* cnt;
+    ScanScratch scan;
+};
+
+// Per-scene CTA ranges of the stages (device arrays of n_scenes + 1 starts).
+enum BatchMap : int {
+    BM_ZERO_FLAGS = 0,  // key_space bytes in 4 KiB pieces
+    BM_PARTICLES,       // particles, 4 per thread (keys, histogram, scatter)
+    BM_KEYSPACE,        // one thread per page key (grid marking, compaction)
+    BM_KEY_TILES,       // scan tiles of the key space
+    BM_LINKS,           // page links
+    BM_ZERO_CELLS,      // cell counters in 4 KiB pieces
+    BM_CELL_TILES,      // scan tiles of the cell counters
+    BM_CANON,
+    BM_P2G,
+    BM_GRID,
+    BM_G2P,
+    BM_ONE,             // one CTA per scene (scan of the tile sums, clock, diagnostics reset)
+    kBatchMaps
+};
+
+struct BatchPlan {
+    int n_scenes;
+    const int32_t* start[kBatchMaps];  // device
+    int total[kBatchMaps];             // CTAs of each launch
+    int deterministic;                 // P2G's fixed-order mode
+    int other_models;                  // a material uses an energy model other than von Mises
+    int fallback;                      // FP32 with the FP64 SVD fallback
+};
+
+// Host-side CTA counts of one scene per map (the same shapes as its one-scene
+// launches; canon, P2G, grid and G2P sized for `sms` SMs).
+void batch_scene_ctas(int64_t n, uint32_t key_space, int nb_cap, int ng_cap, int sms, int real_bytes,
+                      int ctas[kBatchMaps]);
+
+template <typename R>
+cudaError_t launch_batch_binning(const SceneArgs<R>* args, const BatchPlan& plan, cudaStream_t s);
+template <typename R>
+cudaError_t launch_batch_p2g(const SceneArgs<R>* args, const BatchPlan& plan, cudaStream_t s);
+template <typename R>
+cudaError_t launch_batch_grid(const SceneArgs<R>* args, const BatchPlan& plan, cudaStream_t s);
+template <typename R>
+cudaError_t launch_batch_g2p(const SceneArgs<R>* args, const BatchPlan& plan, cudaStream_t s);
+constexpr int kBatchLaunchesPerSubstep = 25;
+
 }  // namespace gmpm

@@ -35,13 +35,13 @@
 
 #include "async_copy.cuh"
 #include "kernels.h"
+#include "launch.cuh"
 
 namespace gmpm {
 
 constexpr int kP2GWarps = 16;  // one per cell z-column (cx, cy)
 constexpr int kP2GThreads = 32 * kP2GWarps;
 constexpr int kColumns = 144;  // 16 cell z-columns x 9 stencil columns
-constexpr int kColAcc = 54;    // 6 z-nodes x 9 channels per stencil column
 // Page flush: column sums channel-major, [channel][stencil column (144)][z (6)], the channel stride padded
 // so that the three channel groups of a warp's stores fall in different banks.  A gather step of one
 // channel over consecutive window nodes then reads consecutive words.
@@ -240,14 +240,17 @@ __device__ __forceinline__ int group_channel(int g, int q) {
     return g == 0 ? CH_CW : (g == 1 ? CH_VW : CH_KC);
 }
 
-// Chunk sequence of one CTA: its pages blockIdx.x + k gridDim.x, each cut
-// into runs of CH slots.  Every thread runs the same iterator.
+// Chunk sequence of one CTA: its pages b + k g (b, g: the CTA's index and the
+// CTA count of its scene's share of the launch), each cut into runs of CH
+// slots.  Every thread runs the same iterator.
 template <int CH>
 struct ChunkIter {
     int page, next, end;  // current page, next run start, page end
     int nbs, nbe;         // slot range of the following page (loaded one page ahead)
-    __device__ void init(const BinDev& bin, int nb) {
-        page = blockIdx.x;
+    int stride;           // CTAs of the scene's share of the launch
+    __device__ void init(const BinDev& bin, int nb, VB vb) {
+        page = vb.b;
+        stride = vb.g;
         next = end = 0;
         if (page < nb) {
             next = bin.cell_start[(int64_t)page * 64];
@@ -256,7 +259,7 @@ struct ChunkIter {
         preload(bin, nb);
     }
     __device__ void preload(const BinDev& bin, int nb) {
-        const int q = page + (int)gridDim.x;
+        const int q = page + stride;
         nbs = nbe = 0;
         if (q < nb) {
             nbs = bin.cell_start[(int64_t)q * 64];
@@ -266,7 +269,7 @@ struct ChunkIter {
     // Next chunk (page, first slot, count, last chunk of its page); count 0 when done.
     __device__ void step(const BinDev& bin, int nb, int& b, int& s0, int& n, int& last) {
         while (page < nb && next >= end) {
-            page += gridDim.x;
+            page += stride;
             next = nbs;
             end = nbe;
             if (page < nb) preload(bin, nb);
@@ -345,9 +348,9 @@ constexpr size_t p2g_stage_bytes() {
 }
 
 template <typename R, bool kDeterministic>
-__global__ void __launch_bounds__(kP2GThreads, 1)
-    k_p2g(const SceneDev<R>* __restrict__ sc, PState<R> st, PAux<R> aux, BinDev bin, R* __restrict__ tile,
-          Counters* __restrict__ cnt) {
+__device__ __forceinline__ void p2g_body(VB vb, const SceneDev<R>* __restrict__ sc, const PState<R>& st,
+                                         const PAux<R>& aux, const BinDev& bin, R* __restrict__ tile,
+                                         Counters* __restrict__ cnt) {
     constexpr int CH = P2GChunk<R>::value;
     constexpr int W = Staging<R>::W, WS = Staging<R>::WS;
     static_assert(sizeof(R) * kP2GChannels * kFlushChStride <= p2g_rec_bytes<R>(), "column sums fit the record buffer");
@@ -377,7 +380,7 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
 
     // prologue: meta of chunks 0 and 1, staging of chunk 0
     ChunkIter<CH> it;
-    it.init(bin, nb);
+    it.init(bin, nb, vb);
     {
         int b0, s0, n0, l0, b1, s1, n1, l1;
         it.step(bin, nb, b0, s0, n0, l0);
@@ -559,6 +562,22 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
     }
 }
 
+template <typename R, bool kDeterministic>
+__global__ void __launch_bounds__(kP2GThreads, 1)
+    k_p2g(const SceneDev<R>* __restrict__ sc, PState<R> st, PAux<R> aux, BinDev bin, R* __restrict__ tile,
+          Counters* __restrict__ cnt) {
+    p2g_body<R, kDeterministic>(own_blocks(), sc, st, aux, bin, tile, cnt);
+}
+
+// Batched launch: the same body for the scene that owns this CTA.
+template <typename R, bool kDeterministic>
+__global__ void __launch_bounds__(kP2GThreads, 1)
+    k_batch_p2g(const SceneArgs<R>* __restrict__ A, const int32_t* __restrict__ start, int ns) {
+    VB vb;
+    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    p2g_body<R, kDeterministic>(vb, a.sc, a.in, a.aux, a.bin, reinterpret_cast<R*>(a.grid.tile), a.cnt);
+}
+
 template <typename R>
 size_t p2g_smem_bytes() {
     return p2g_rec_bytes<R>() + p2g_stage_bytes<R>() + sizeof(P2GMeta<P2GChunk<R>::value>);
@@ -566,12 +585,27 @@ size_t p2g_smem_bytes() {
 
 template <typename R>
 cudaError_t prepare_p2g() {
-    cudaError_t e = cudaFuncSetAttribute(k_p2g<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)p2g_smem_bytes<R>());
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_p2g<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)p2g_smem_bytes<R>());
+    const int smem = (int)p2g_smem_bytes<R>();
+    cudaError_t e = cudaFuncSetAttribute(k_p2g<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_p2g<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_p2g<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_p2g<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
 }
+
+template <typename R>
+cudaError_t launch_batch_p2g(const SceneArgs<R>* A, const BatchPlan& P, cudaStream_t s) {
+    const dim3 grid((unsigned)P.total[BM_P2G]);
+    if (P.deterministic)
+        return launch_kernel(k_batch_p2g<R, true>, grid, dim3(kP2GThreads), p2g_smem_bytes<R>(), s, A, P.start[BM_P2G],
+                             P.n_scenes);
+    return launch_kernel(k_batch_p2g<R, false>, grid, dim3(kP2GThreads), p2g_smem_bytes<R>(), s, A, P.start[BM_P2G],
+                         P.n_scenes);
+}
+template cudaError_t launch_batch_p2g<float>(const SceneArgs<float>*, const BatchPlan&, cudaStream_t);
+template cudaError_t launch_batch_p2g<double>(const SceneArgs<double>*, const BatchPlan&, cudaStream_t);
 template cudaError_t prepare_p2g<float>();
 template cudaError_t prepare_p2g<double>();
 

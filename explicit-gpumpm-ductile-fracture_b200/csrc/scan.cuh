@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "common.cuh"
 #include "launch.cuh"
 
 namespace gmpm {
@@ -55,10 +56,12 @@ __device__ __forceinline__ int32_t block_exclusive_sum(int32_t x, int32_t* total
     return r;
 }
 
+// Bodies take the CTA's tile index within its scene's scan (VB, common.cuh),
+// so that the same code serves one-scene and batched launches.
 template <typename TIn>
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const TIn* __restrict__ in, int64_t n,
-                                                               int32_t* __restrict__ tile_sums) {
-    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+__device__ __forceinline__ void scan_reduce_body(VB vb, const TIn* __restrict__ in, int64_t n,
+                                                 int32_t* __restrict__ tile_sums) {
+    const int64_t base = (int64_t)vb.b * kScanTile + (int64_t)threadIdx.x * kScanItems;
     int32_t v[kScanItems];
     scan_load(in, n, base, v);
     int32_t s = 0;
@@ -66,12 +69,18 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const TIn* __restr
     for (int q = 0; q < kScanItems; ++q) s += v[q];
     __shared__ int32_t tot;
     block_exclusive_sum(s, &tot);
-    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+    if (threadIdx.x == 0) tile_sums[vb.b] = tot;
+}
+
+template <typename TIn>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const TIn* __restrict__ in, int64_t n,
+                                                               int32_t* __restrict__ tile_sums) {
+    scan_reduce_body(own_blocks(), in, n, tile_sums);
 }
 
 // Single CTA: exclusive scan of the tile sums in place, total to *total.
-static __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t* __restrict__ tile_sums, int64_t ntiles,
-                                                              int32_t* __restrict__ total) {
+__device__ __forceinline__ void scan_tiles_body(int32_t* __restrict__ tile_sums, int64_t ntiles,
+                                                int32_t* __restrict__ total) {
     __shared__ int32_t chunk_total;
     int32_t carry = 0;
     for (int64_t base = 0; base < ntiles; base += kScanTile) {
@@ -93,23 +102,34 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t* __r
     if (threadIdx.x == 0) *total = carry;
 }
 
+static __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t* __restrict__ tile_sums, int64_t ntiles,
+                                                              int32_t* __restrict__ total) {
+    scan_tiles_body(tile_sums, ntiles, total);
+}
+
 template <typename TIn>
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const TIn* __restrict__ in, int64_t n,
-                                                              const int32_t* __restrict__ tile_offsets,
-                                                              int32_t* __restrict__ out) {
-    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+__device__ __forceinline__ void scan_apply_body(VB vb, const TIn* __restrict__ in, int64_t n,
+                                                const int32_t* __restrict__ tile_offsets, int32_t* __restrict__ out) {
+    const int64_t base = (int64_t)vb.b * kScanTile + (int64_t)threadIdx.x * kScanItems;
     int32_t v[kScanItems];
     scan_load(in, n, base, v);
     int32_t s = 0;
 #pragma unroll
     for (int q = 0; q < kScanItems; ++q) s += v[q];
     __shared__ int32_t tot;
-    int32_t run = block_exclusive_sum(s, &tot) + tile_offsets[blockIdx.x];
+    int32_t run = block_exclusive_sum(s, &tot) + tile_offsets[vb.b];
 #pragma unroll
     for (int q = 0; q < kScanItems; ++q) {
         if (base + q < n) out[base + q] = run;
         run += v[q];
     }
+}
+
+template <typename TIn>
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const TIn* __restrict__ in, int64_t n,
+                                                              const int32_t* __restrict__ tile_offsets,
+                                                              int32_t* __restrict__ out) {
+    scan_apply_body(own_blocks(), in, n, tile_offsets, out);
 }
 
 // out[i] = sum_{j<i} in[j] for i < n; *total = sum of all.  Returns the

@@ -46,10 +46,20 @@ struct SceneBase {
     virtual int parity() const = 0;
     virtual int kernels_per_substep() const = 0;
     virtual gmpm_status launch_substep(cudaStream_t s, int parity) = 0;
-    virtual void commit_substeps(int n) = 0;
+    // own_launches: the substeps ran the scene's own kernels (a branch or the
+    // plain path), not a batch's launches over many scenes.
+    virtual void commit_substeps(int n, bool own_launches = true) = 0;
     // Launch shapes are sized for this many SMs (0: the whole device).
     virtual void set_sm_share(int sms) = 0;
     virtual int sm_share() const = 0;
+    // One launch per stage over many scenes (kernels.h, BatchPlan): the kind of
+    // the scene's kernels (precision, P2G mode, energy models, FP64 fallback;
+    // -1 if the scene cannot join, as with the implicit phase field), its
+    // buffers for a parity as a SceneArgs<R> (into out), and the sizes that
+    // set its CTA ranges.
+    virtual int batch_kind() const = 0;
+    virtual void batch_args(int parity, void* out) const = 0;
+    virtual void batch_sizes(int64_t* n, uint32_t* key_space, int* nb_cap, int* ng_cap) const = 0;
 
     // Checkpoint of the particle state and clock (gmpm_scene_save).
     virtual gmpm_status save(const char* path) = 0;

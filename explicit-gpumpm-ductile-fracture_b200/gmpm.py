@@ -116,7 +116,8 @@ class BatchInfo(C.Structure):
                 ("graph_nodes", C.c_int64), ("captures", C.c_int64), ("substeps", C.c_int64),
                 ("best_ms_per_substep", C.c_double), ("sm_share_small", C.c_int32),
                 ("sm_share_medium", C.c_int32), ("sm_share_large", C.c_int32), ("_pad0", C.c_int32),
-                ("capture_seconds", C.c_double)]
+                ("capture_seconds", C.c_double), ("kernel_nodes", C.c_int64), ("table_scenes", C.c_int32),
+                ("_pad1", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}

@@ -444,11 +444,14 @@ gmpm_status gmpm_scene_load(gmpm_context* ctx, const char* path, gmpm_scene** ou
 /* ---- Batched stepping of independent scenes --------------------------------------------------
  * No reference counterpart: the reference steps one scene per MPMSimulator::simulateStick call
  * (Simulator.cpp:227-259).  A batch advances many independent scenes of uneven size, each with its
- * own grid, with one CUDA graph launch per substep; every scene's binning, P2G, grid update and G2P
- * is a parallel branch of that graph.  Each scene's results are the same as stepping it alone
- * (bitwise in deterministic mode).  The autotuner times candidate launch shapes (the share of SMs
- * each scene's kernels are sized for, per scene size class, and the number of concurrent branches)
- * on the first substeps, which are real substeps, and keeps the fastest.
+ * own grid, with one CUDA graph launch per substep.  Scenes whose kernels are of one kind (precision,
+ * P2G mode, energy models, FP64 fallback) advance together with one launch per stage of the substep
+ * over a device table of the scenes (25 launches per kind, whatever the number of scenes); scenes
+ * with the implicit phase field run their own launch sequences on parallel branches of the graph.
+ * Each scene's results are the same as stepping it alone (bitwise in deterministic mode).  The
+ * autotuner times candidate launch shapes (the share of SMs each scene's page- and slot-parallel
+ * stages are sized for, per scene size class, and the number of concurrent branches) on the first
+ * substeps, which are real substeps, and keeps the fastest.
  * Destroy a batch before any of its scenes; a scene may belong to several batches. */
 typedef struct gmpm_batch gmpm_batch;
 
@@ -473,6 +476,9 @@ typedef struct gmpm_batch_info {
     int32_t sm_share_large;   /* ... 200,000 particles and above */
     int32_t _pad0;
     double capture_seconds;   /* host time spent capturing and instantiating graphs */
+    int64_t kernel_nodes;     /* kernel launches of one substep graph */
+    int32_t table_scenes;     /* scenes advanced by one launch per stage (the rest on branches) */
+    int32_t _pad1;
 } gmpm_batch_info;
 
 void gmpm_batch_options_defaults(gmpm_batch_options* opt);

@@ -72,3 +72,52 @@ def test_batched_workload_scene_stays_finite(pkg, ctx):
     sc = sp.build(ctx)
     sc.substep(40)
     assert sc.sync() == G.OK
+
+
+def test_batch_is_one_launch_per_stage_over_its_scenes(pkg, ctx):
+    """Scenes of one kernel kind advance with one launch per stage, so the
+    graph's kernel count depends on the kinds present, not on the number of
+    scenes: 40 bars of one kind give the same 25 kernel nodes as 3."""
+    G, S = pkg.gmpm, pkg.scenes
+    nodes = {}
+    for count in (3, 40):
+        specs = S.notched_bar_batch(count, seed=3, lo=4_000, hi=30_000, substeps=4)
+        scenes = [sp.build(ctx) for sp in specs]
+        batch = G.Batch(ctx, scenes, autotune=False)
+        batch.substep(4)
+        info = batch.info()
+        assert info["table_scenes"] == count
+        nodes[count] = info["kernel_nodes"]
+        if count == 40:  # two of them against the same scenes alone
+            for k in (0, 27):
+                alone = specs[k].build(ctx)
+                alone.substep(4)
+                _same(alone, scenes[k], specs[k].name)
+                alone.close()
+        batch.close()
+        for sc in scenes:
+            sc.close()
+    assert nodes[3] == nodes[40] == 25
+
+
+def test_batch_with_implicit_scene_on_a_branch(pkg, ctx):
+    """A scene with the implicit phase field (its solve stops on a device flag)
+    runs its own launch sequence on a branch beside the scene table; both
+    kinds of scene still end equal to themselves alone."""
+    G, S = pkg.gmpm, pkg.scenes
+    specs = S.notched_bar_batch(3, seed=9, lo=6_000, hi=20_000, substeps=6)
+    imp = S.notched_bar_sized(10_000, seed=5, precision=G.PRECISION_FP64, substeps=6)
+    imp.desc.phase_field = G.PHASE_FIELD_IMPLICIT
+    specs.append(imp)
+    alone = [sp.build(ctx) for sp in specs]
+    mixed = [sp.build(ctx) for sp in specs]
+    for sc in alone:
+        sc.substep(6)
+    batch = G.Batch(ctx, mixed, autotune=False)
+    batch.substep(6)
+    info = batch.info()
+    assert info["table_scenes"] == 3 and info["kernel_nodes"] > 25
+    for sp, a, b in zip(specs, alone, mixed):
+        assert a.sync() == G.OK and b.sync() == G.OK
+        _same(a, b, sp.name)
+    batch.close()
