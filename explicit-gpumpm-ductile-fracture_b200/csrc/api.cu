@@ -265,12 +265,14 @@ struct Scene : SceneBase {
     size_t staging_bytes = 0;
     std::vector<void*> allocs;
     bool binned = false;  // binning of the current positions is valid
+    // bin.keys and bin.page_flag hold the keys and pages of the current
+    // positions (set by a key pass or by the G2P that wrote them), so the next
+    // binning skips its key pass
+    bool keys_fresh = false;
     int64_t launches = 0;  // kernels launched by this scene
     uint64_t uid_ = g_scene_uid++;
     int share_ = 0;        // SMs the launch shapes are sized for (0: all)
     size_t dev_bytes_ = 0;
-    // kernels per launch_binning: keys, 3 scans x 3, mark, 2 compactions, links, hist, scatter, canon
-    static constexpr int kBinningKernels = 17;
 
     // Device memory comes from the device's stream-ordered pool.  A scene
     // released on a stream (the serving loop, after its last use there) frees
@@ -493,6 +495,9 @@ struct Scene : SceneBase {
         GMPM_TRY(prepare_p2g<R>());
         GMPM_TRY(prepare_g2p<R>());
         GMPM_TRY(cudaMemset(d_cnt, 0, sizeof(Counters)));
+        // keys of the initial positions into the cleared counters (an
+        // out-of-domain particle raises its flag here)
+        GMPM_TRY(refresh_keys(0));
         // creation work ran on the legacy stream; waiting for it alone leaves
         // other streams' work (e.g. a serving batch) running
         GMPM_TRY(cudaStreamSynchronize(0));
@@ -520,9 +525,25 @@ struct Scene : SceneBase {
     void launch_keys_only(cudaStream_t s);
     void mark_grid(cudaStream_t s);
 
+    // A key pass over the current positions: keys and page flags.
+    cudaError_t refresh_keys(cudaStream_t s) {
+        cudaError_t e = cudaMemsetAsync(bin.page_flag, 0, bin.key_space, s);
+        if (e == cudaSuccess) e = launch_keys<R>(d_sc, st[cur], bin, d_cnt, s);
+        if (e == cudaSuccess) keys_fresh = true;
+        return e;
+    }
+    gmpm_status ensure_keys(cudaStream_t s) override {
+        if (keys_fresh) return GMPM_OK;
+        GMPM_TRY(cudaSetDevice(ctx->device));
+        launches += 1;
+        GMPM_TRY(refresh_keys(s));
+        return GMPM_OK;
+    }
+
     gmpm_status do_bin(cudaStream_t s) {
         GMPM_TRY(launch_binning<R>(d_sc, st[cur], bin, scan, d_cnt, cfg().num_sms, s));
         binned = true;
+        keys_fresh = true;
         return GMPM_OK;
     }
 
@@ -533,8 +554,10 @@ struct Scene : SceneBase {
     gmpm_status launch_one(cudaStream_t s, int c, cudaEvent_t* ev, bool host_checks = true,
                            int64_t* kernels = nullptr) {
         const LaunchCfg lc = cfg();
-        int64_t nk = kBinningKernels + 4;
-        GMPM_TRY(launch_binning<R>(d_sc, st[c], bin, scan, d_cnt, lc.num_sms, s));
+        const bool keys_ready = keys_fresh;
+        keys_fresh = false;  // until this substep's G2P has keyed the new positions
+        int64_t nk = (keys_ready ? kBinningKernelsKeysReady : kBinningKernels) + 4;
+        GMPM_TRY(launch_binning<R>(d_sc, st[c], bin, scan, d_cnt, lc.num_sms, s, keys_ready));
         if (ev) GMPM_TRY(cudaEventRecord(ev[0], s));
         GMPM_TRY(launch_p2g<R>(d_sc, st[c], aux, bin, grid, d_cnt, lc, s));
         if (ev) GMPM_TRY(cudaEventRecord(ev[1], s));
@@ -558,6 +581,7 @@ struct Scene : SceneBase {
         if (ev) GMPM_TRY(cudaEventRecord(ev[2], s));
         GMPM_TRY(launch_g2p<R>(d_sc, d_sc64, desc.precision == GMPM_PRECISION_FP32_FP64SVD ? d_sc64 : nullptr,
                                st[c], st[1 - c], aux, bin, grid, d_cnt, lc, s));
+        keys_fresh = true;
         if (ev) GMPM_TRY(cudaEventRecord(ev[3], s));
         return GMPM_OK;
     }
@@ -578,7 +602,7 @@ struct Scene : SceneBase {
     size_t device_bytes() const override { return dev_bytes_; }
     int parity() const override { return cur; }
     int kernels_per_substep() const override {
-        return kBinningKernels + 4 +
+        return kBinningKernelsKeysReady + 4 +
                (implicit_pf() ? kPcgInitKernels + kPcgFinishKernels + desc.pcg_max_iterations * kPcgIterationKernels
                               : 0);
     }
@@ -681,6 +705,7 @@ struct Scene : SceneBase {
         const R dtr = (R)h.dt;
         GMPM_TRY(cudaMemcpy(&d_sc->dt, &dtr, sizeof(R), cudaMemcpyHostToDevice));
         GMPM_TRY(cudaMemcpy(&d_sc64->dt, &h.dt, sizeof(double), cudaMemcpyHostToDevice));
+        GMPM_TRY(refresh_keys(0));
         GMPM_TRY(cudaDeviceSynchronize());
         binned = false;
         return GMPM_OK;

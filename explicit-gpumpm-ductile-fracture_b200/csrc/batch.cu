@@ -7,7 +7,7 @@
 // energy models, FP64 fallback) form a group, and the group's substep is one
 // launch per stage over all its scenes (launch_batch_*, kernels.h): a device
 // array of the scenes' buffers and, per stage, each scene's range of CTAs.
-// A graph therefore holds the same 25 kernel nodes per group whatever the
+// A graph therefore holds the same 23 kernel nodes per group whatever the
 // number of scenes, and small scenes' stages fill the device together.
 // Scenes that cannot join a group (the implicit phase field, whose solve
 // stops on a device flag) are captured as their own launch sequences on
@@ -342,6 +342,11 @@ struct Batch {
             release_graphs();
             parity0.resize(sc.size());
             for (size_t i = 0; i < sc.size(); ++i) parity0[i] = sc[i]->parity();
+            // the captured substeps skip the key pass (G2P keys the positions it writes)
+            for (SceneBase* s : sc) {
+                gmpm_status r = s->ensure_keys(cap);
+                if (r != GMPM_OK) return r;
+            }
             gmpm_status r = prepare_tables();
             if (r != GMPM_OK) return r;
             r = capture(0, &exec[0]);
@@ -362,6 +367,8 @@ struct Batch {
         for (int it = 0; it < n; ++it) {
             int k = 0;
             gmpm_status r = ensure_graphs(&k);
+            // positions written since the last substep other than by a G2P get their keys
+            for (size_t i = 0; i < sc.size() && r == GMPM_OK; ++i) r = sc[i]->ensure_keys(s);
             if (r != GMPM_OK) return r;
             BATCH_TRY(cudaGraphLaunch(exec[k], s));
             BATCH_TRY(cudaEventRecord(last, s));

@@ -33,9 +33,7 @@ __device__ __forceinline__ void bin_keys_body(VB vb, int64_t n, const R* __restr
                                               Counters* cnt) {
     const int64_t i0 = (int64_t)vb.b * kBinThreads * kBinILP + threadIdx.x;
     const double inv_dx = sc->inv_dx_d;
-    int hi[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) hi[a] = sc->res[a] - 3;
+    const int res[3] = {sc->res[0], sc->res[1], sc->res[2]};
     R xs[kBinILP][3];
 #pragma unroll
     for (int u = 0; u < kBinILP; ++u) {
@@ -51,26 +49,9 @@ __device__ __forceinline__ void bin_keys_body(VB vb, int64_t n, const R* __restr
     for (int u = 0; u < kBinILP; ++u) {
         const int64_t i = i0 + (int64_t)u * kBinThreads;
         if (i >= n) continue;
-        int base[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            // (int)(x / dx + 0.5) - 1 as in cal_cellId (Particle_kernal.cu:162-164),
-            // valid when the 3-node stencil stays inside the grid.
-            const double t = __dadd_rn(__dmul_rn((double)xs[u][a], inv_dx), 0.5);
-            if (!(t >= 1.0)) {
-                base[a] = 0;
-                bad = true;
-            } else if (t >= (double)(hi[a] + 2)) {
-                base[a] = hi[a];
-                bad = true;
-            } else {
-                base[a] = (int)t - 1;
-            }
-        }
-        const uint32_t cell = (uint32_t)(((base[0] & 3) << 4) | ((base[1] & 3) << 2) | (base[2] & 3));
-        const uint32_t pk = page_key(base[0] >> 2, base[1] >> 2, base[2] >> 2);
-        keys[i] = (pk << 6) | cell;
-        page_flag[pk] = 1;
+        const uint32_t key = cell_key(xs[u], inv_dx, res, bad);
+        keys[i] = key;
+        page_flag[key >> 6] = 1;
     }
     if (bad) raise_flag(cnt, GMPM_FLAG_OUT_OF_DOMAIN);
 }
@@ -347,14 +328,16 @@ cudaError_t launch_bin_canon(BinDev bin, Counters* cnt, int num_sms, cudaStream_
 
 template <typename R>
 cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bin, ScanScratch scan, Counters* cnt,
-                           int num_sms, cudaStream_t stream) {
+                           int num_sms, cudaStream_t stream, bool keys_ready) {
     const int64_t n = bin.n;
     const int T = 256;
     const unsigned gn = bin_grid(n);
     const unsigned gk = (bin.key_space + T - 1) / T;
-    cudaMemsetAsync(bin.page_flag, 0, bin.key_space, stream);
     cudaMemsetAsync(bin.grid_flag, 0, bin.key_space, stream);
-    k_bin_keys<R><<<gn, kBinThreads, 0, stream>>>(n, st.x[0], st.x[1], st.x[2], sc, bin.keys, bin.page_flag, cnt);
+    if (!keys_ready) {
+        cudaMemsetAsync(bin.page_flag, 0, bin.key_space, stream);
+        k_bin_keys<R><<<gn, kBinThreads, 0, stream>>>(n, st.x[0], st.x[1], st.x[2], sc, bin.keys, bin.page_flag, cnt);
+    }
     scan_exclusive<uint8_t>(bin.page_flag, bin.page_rank, (int64_t)bin.key_space, &cnt->n_blocks, scan, stream);
     k_mark_grid<<<gk, T, 0, stream>>>(bin.key_space, bin.page_flag, bin.grid_flag);
     scan_exclusive<uint8_t>(bin.grid_flag, bin.grid_rank, (int64_t)bin.key_space, &cnt->n_grid_blocks, scan, stream);
@@ -362,6 +345,8 @@ cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bi
     k_compact_keys<<<gk, T, 0, stream>>>(bin.key_space, bin.grid_flag, bin.grid_rank, bin.grid_keys, bin.ng_cap, cnt);
     const int links = max(bin.nb_cap, bin.ng_cap) * 8;
     k_page_links<<<(links + T - 1) / T, T, 0, stream>>>(bin, cnt);
+    // the page flags' last use was the links: cleared for the G2P that keys the next positions
+    if (keys_ready) cudaMemsetAsync(bin.page_flag, 0, bin.key_space, stream);
     const int64_t ncell = (int64_t)bin.nb_cap * 64;
     cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), stream);
     launch_bin_hist(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap, stream);
@@ -411,34 +396,31 @@ void batch_scene_ctas(int64_t n, uint32_t key_space, int nb_cap, int ng_cap, int
     ctas[BM_ONE] = 1;
 }
 
-// Zero `bytes` (a multiple of 4) from p: 4 KiB per CTA.
+// Zero `bytes` (a multiple of 4) from p in 4 KiB pieces: pieces vb.b, vb.b + vb.g, ...
 __device__ __forceinline__ void zero_bytes_body(VB vb, void* p, int64_t bytes) {
     char* c = static_cast<char*>(p);
-    const int64_t off = (int64_t)vb.b * 4096 + (int64_t)threadIdx.x * 16;
-    if (off + 16 <= bytes && ((reinterpret_cast<uintptr_t>(c) & 15) == 0)) {
-        *reinterpret_cast<uint4*>(c + off) = make_uint4(0u, 0u, 0u, 0u);
-    } else {
-        for (int q = 0; q < 16; q += 4)
-            if (off + q + 4 <= bytes) *reinterpret_cast<uint32_t*>(c + off + q) = 0u;
+    const bool aligned = (reinterpret_cast<uintptr_t>(c) & 15) == 0;
+    for (int64_t piece = (int64_t)vb.b * 4096; piece < bytes; piece += (int64_t)vb.g * 4096) {
+        const int64_t off = piece + (int64_t)threadIdx.x * 16;
+        if (off + 16 <= bytes && aligned) {
+            *reinterpret_cast<uint4*>(c + off) = make_uint4(0u, 0u, 0u, 0u);
+        } else {
+            for (int q = 0; q < 16; q += 4)
+                if (off + q + 4 <= bytes) *reinterpret_cast<uint32_t*>(c + off + q) = 0u;
+        }
     }
 }
 
+// which: 1 grid flags; 2 cell counters; 3 cell counters and page flags (after
+// the page flags' last use in the binning, for the G2P that sets them).
 template <typename R>
 __global__ void __launch_bounds__(256) k_batch_zero(const SceneArgs<R>* __restrict__ A, const int32_t* __restrict__ start,
                                                     int ns, int which) {
     VB vb;
     const BinDev& bin = A[scene_of_block(start, ns, vb)].bin;
-    if (which == 0) zero_bytes_body(vb, bin.page_flag, bin.key_space);
     if (which == 1) zero_bytes_body(vb, bin.grid_flag, bin.key_space);
-    if (which == 2) zero_bytes_body(vb, bin.cell_count, (int64_t)bin.nb_cap * 64 * 4);
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kBinThreads) k_batch_keys(const SceneArgs<R>* __restrict__ A,
-                                                            const int32_t* __restrict__ start, int ns) {
-    VB vb;
-    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
-    bin_keys_body<R>(vb, a.bin.n, a.in.x[0], a.in.x[1], a.in.x[2], a.sc, a.bin.keys, a.bin.page_flag, a.cnt);
+    if (which >= 2) zero_bytes_body(vb, bin.cell_count, (int64_t)bin.nb_cap * 64 * 4);
+    if (which == 3) zero_bytes_body(vb, bin.page_flag, bin.key_space);
 }
 
 // The three scans of the binning: 0 page flags -> page ranks, 1 grid flags ->
@@ -548,16 +530,14 @@ __global__ void __launch_bounds__(32 * kCanonWarps) k_batch_canon(const SceneArg
     bin_canon_body(vb, a.bin, a.cnt);
 }
 
-// The binning of every scene of a batch: the same steps as launch_binning,
-// each one launch over all scenes.
+// The binning of every scene of a batch: the same steps as launch_binning with
+// keys_ready, each one launch over all scenes.
 template <typename R>
 cudaError_t launch_batch_binning(const SceneArgs<R>* A, const BatchPlan& P, cudaStream_t s) {
     const int ns = P.n_scenes;
     auto T = [&](int m) { return dim3((unsigned)P.total[m]); };
     auto S = [&](int m) { return P.start[m]; };
-    cudaError_t e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_FLAGS), dim3(256), 0, s, A, S(BM_ZERO_FLAGS), ns, 0);
-    if (e == cudaSuccess) e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_FLAGS), dim3(256), 0, s, A, S(BM_ZERO_FLAGS), ns, 1);
-    if (e == cudaSuccess) e = launch_kernel(k_batch_keys<R>, T(BM_PARTICLES), dim3(kBinThreads), 0, s, A, S(BM_PARTICLES), ns);
+    cudaError_t e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_FLAGS), dim3(256), 0, s, A, S(BM_ZERO_FLAGS), ns, 1);
     if (e == cudaSuccess) e = launch_kernel(k_batch_scan_reduce<R, 0>, T(BM_KEY_TILES), dim3(kScanThreads), 0, s, A, S(BM_KEY_TILES), ns);
     if (e == cudaSuccess) e = launch_kernel(k_batch_scan_tiles<R, 0>, T(BM_ONE), dim3(kScanThreads), 0, s, A, S(BM_ONE), ns);
     if (e == cudaSuccess) e = launch_kernel(k_batch_scan_apply<R, 0>, T(BM_KEY_TILES), dim3(kScanThreads), 0, s, A, S(BM_KEY_TILES), ns);
@@ -567,7 +547,7 @@ cudaError_t launch_batch_binning(const SceneArgs<R>* A, const BatchPlan& P, cuda
     if (e == cudaSuccess) e = launch_kernel(k_batch_scan_apply<R, 1>, T(BM_KEY_TILES), dim3(kScanThreads), 0, s, A, S(BM_KEY_TILES), ns);
     if (e == cudaSuccess) e = launch_kernel(k_batch_compact<R>, T(BM_KEYSPACE), dim3(256), 0, s, A, S(BM_KEYSPACE), ns);
     if (e == cudaSuccess) e = launch_kernel(k_batch_links<R>, T(BM_LINKS), dim3(256), 0, s, A, S(BM_LINKS), ns);
-    if (e == cudaSuccess) e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_CELLS), dim3(256), 0, s, A, S(BM_ZERO_CELLS), ns, 2);
+    if (e == cudaSuccess) e = launch_kernel(k_batch_zero<R>, T(BM_ZERO_CELLS), dim3(256), 0, s, A, S(BM_ZERO_CELLS), ns, 3);
     if (e == cudaSuccess) e = launch_kernel(k_batch_hist<R>, T(BM_PARTICLES), dim3(kBinThreads), 0, s, A, S(BM_PARTICLES), ns);
     if (e == cudaSuccess) e = launch_kernel(k_batch_scan_reduce<R, 2>, T(BM_CELL_TILES), dim3(kScanThreads), 0, s, A, S(BM_CELL_TILES), ns);
     if (e == cudaSuccess) e = launch_kernel(k_batch_scan_tiles<R, 2>, T(BM_ONE), dim3(kScanThreads), 0, s, A, S(BM_ONE), ns);
@@ -581,8 +561,8 @@ template cudaError_t launch_batch_binning<float>(const SceneArgs<float>*, const 
 template cudaError_t launch_batch_binning<double>(const SceneArgs<double>*, const BatchPlan&, cudaStream_t);
 
 template cudaError_t launch_binning<float>(const SceneDev<float>*, const PState<float>&, BinDev, ScanScratch,
-                                           Counters*, int, cudaStream_t);
+                                           Counters*, int, cudaStream_t, bool);
 template cudaError_t launch_binning<double>(const SceneDev<double>*, const PState<double>&, BinDev, ScanScratch,
-                                            Counters*, int, cudaStream_t);
+                                            Counters*, int, cudaStream_t, bool);
 
 }  // namespace gmpm

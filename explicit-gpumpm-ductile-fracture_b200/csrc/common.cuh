@@ -132,6 +132,32 @@ __host__ __device__ inline void page_coords(uint32_t key, int& bx, int& by, int&
 
 __device__ inline void raise_flag(Counters* c, unsigned int f) { atomicOr(&c->flags, f); }
 
+// Cell key of a position, (page_key << 6) | cell of the base node, with the
+// base node (int)(x / dx + 0.5) - 1 in FP64 as in cal_cellId
+// (Particle_kernal.cu:162-164).  A base node whose 3-node stencil would leave
+// the grid is clamped to its edge and sets `bad`.  Shared by the binning's key
+// pass and G2P, which keys the positions it writes.
+template <typename R>
+__device__ __forceinline__ uint32_t cell_key(const R x[3], double inv_dx, const int res[3], bool& bad) {
+    int base[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int hi = res[a] - 3;
+        const double t = __dadd_rn(__dmul_rn((double)x[a], inv_dx), 0.5);
+        if (!(t >= 1.0)) {
+            base[a] = 0;
+            bad = true;
+        } else if (t >= (double)(hi + 2)) {
+            base[a] = hi;
+            bad = true;
+        } else {
+            base[a] = (int)t - 1;
+        }
+    }
+    const uint32_t cell = (uint32_t)(((base[0] & 3) << 4) | ((base[1] & 3) << 2) | (base[2] & 3));
+    return (page_key(base[0] >> 2, base[1] >> 2, base[2] >> 2) << 6) | cell;
+}
+
 // ---- launches over one scene or many ------------------------------------------
 // A kernel body sees its CTA's index and the CTA count of its scene's share of
 // the launch: the CUDA block index and grid size in a one-scene launch, or the

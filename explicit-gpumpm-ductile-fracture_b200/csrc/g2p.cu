@@ -9,7 +9,10 @@
 // particle then gathers its 3x3x3 stencil, updates c
 // (irreversibly), x, F = (I + dt grad v) F, the APIC matrix B, runs the SVD +
 // Hencky return map + damage driving force, and writes the particle in the
-// new sorted order.  Reading the previous order through perm and writing the
+// new sorted order, with the cell key and page flag of its new position for
+// the next substep's binning (cal_cellId, Particle_kernal.cu:158-165, done
+// where the position is written instead of in a pass that reads it back).
+// Reading the previous order through perm and writing the
 // new order is the reorder the reference does with gathers and D2D copies
 // (Particle_kernal.cu:544-573, TimeIntegrator.cu:459-461).
 #include <algorithm>
@@ -62,6 +65,10 @@ struct G2PShared {
     // per window value w = ch * 216 + node: source offset in its grid page
     // (bits 0-8), neighbour slot (9-11), destination offset (12-21), c_new flag (22)
     uint32_t wtab[kGridChannels * kWindowNodes];
+    // the cell-key parameters, read where each particle's key is formed (not
+    // held in registers across the loop)
+    double key_inv_dx;
+    int key_res[3];
 };
 
 enum : int { P_X = 0, P_C = 3, P_M = 4 };
@@ -418,6 +425,8 @@ __device__ __forceinline__ void g2p_body(VB vb, const SceneDev<R>* __restrict__ 
             S.unit[0][q] = d0[q];
             S.unit[1][q] = d1[q];
         }
+        S.key_inv_dx = sc->inv_dx_d;
+        for (int a = 0; a < 3; ++a) S.key_res[a] = sc->res[a];
     }
     issue_meta(S, 0, d0[0], d0[1], d0[2], d0[3], d0[6], bin);
     cp_async_commit();
@@ -492,12 +501,22 @@ __device__ __forceinline__ void g2p_body(VB vb, const SceneDev<R>* __restrict__ 
             const R c_new = fmax(fmin(c_old, c_old + dcp), R(0));
             // Write the transfer results first so they are dead during the SVD.
             bool finite = true;
+            R xn[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                const R xn = x[a] + vp[a] * dt;
-                out.x[a][slot] = xn;
+                xn[a] = x[a] + vp[a] * dt;
+                out.x[a][slot] = xn[a];
                 aux.v[a][slot] = vp[a];
-                finite = finite && isfinite(xn);
+                finite = finite && isfinite(xn[a]);
+            }
+            {
+                // the new position's cell key and page, which the next
+                // substep's binning reads instead of running its key pass
+                bool bad = false;
+                const uint32_t key = cell_key(xn, S.key_inv_dx, S.key_res, bad);
+                bin.keys[slot] = key;
+                bin.page_flag[key >> 6] = 1;
+                if (bad) flags |= GMPM_FLAG_OUT_OF_DOMAIN;
             }
 #pragma unroll
             for (int q = 0; q < 9; ++q) aux.B[q][slot] = Bn[q];

@@ -158,8 +158,9 @@ __global__ void __launch_bounds__(kGridThreads)
 template <typename R>
 __global__ void __launch_bounds__(kGridThreads)
     k_batch_grid(const SceneArgs<R>* __restrict__ A, const int32_t* __restrict__ start, int ns) {
+    __shared__ SceneArgs<R> sa;
     VB vb;
-    const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
+    const SceneArgs<R>& a = batch_scene_args(A, start, ns, vb, sa);
     grid_body<R>(vb, a.sc, a.bin, reinterpret_cast<const R*>(a.grid.tile), reinterpret_cast<R*>(a.grid.nodes),
                  a.grid.diag, a.grid.pcg, a.cnt);
 }

@@ -51,9 +51,16 @@ struct LaunchCfg {
     int other_models;      // a material uses an energy model other than von Mises
 };
 
+// keys_ready: bin.keys and bin.page_flag already hold the keys and pages of
+// st's positions (written by the G2P that produced them), so the key pass is
+// skipped and the page flags are cleared after their last use, for the next
+// G2P to set.  Otherwise the key pass runs and the flags stay set.
 template <typename R>
 cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bin, ScanScratch scan, Counters* cnt,
-                           int num_sms, cudaStream_t stream);
+                           int num_sms, cudaStream_t stream, bool keys_ready = false);
+// Kernels launched by launch_binning without / with keys_ready.
+constexpr int kBinningKernels = 17;
+constexpr int kBinningKernelsKeysReady = 16;
 
 // Keys + page flags only, and grid-page marking (used to size capacities).
 template <typename R>
@@ -140,14 +147,33 @@ struct SceneArgs {
     ScanScratch scan;
 };
 
+// The scene of this CTA in a batched launch, with its SceneArgs copied into
+// `sa` (a __shared__ variable of the kernel).  A one-scene kernel reads its
+// buffers' addresses from the constant bank where it uses them; a batched
+// body given references into A keeps them live in registers across its
+// loops.  Reading them from `sa` removes the grid body's spills.  The P2G and
+// G2P bodies spill as much or more with the copy, and read A.
+template <typename R>
+__device__ __forceinline__ const SceneArgs<R>& batch_scene_args(const SceneArgs<R>* __restrict__ A,
+                                                                const int32_t* __restrict__ start, int ns, VB& vb,
+                                                                SceneArgs<R>& sa) {
+    static_assert(sizeof(SceneArgs<R>) % 4 == 0, "copied in 4-byte words");
+    const int s = scene_of_block(start, ns, vb);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&A[s]);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+    for (int w = (int)threadIdx.x; w < (int)(sizeof(SceneArgs<R>) / 4); w += (int)blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    return sa;
+}
+
 // Per-scene CTA ranges of the stages (device arrays of n_scenes + 1 starts).
 enum BatchMap : int {
     BM_ZERO_FLAGS = 0,  // key_space bytes in 4 KiB pieces
-    BM_PARTICLES,       // particles, 4 per thread (keys, histogram, scatter)
+    BM_PARTICLES,       // particles, 4 per thread (histogram, scatter)
     BM_KEYSPACE,        // one thread per page key (grid marking, compaction)
     BM_KEY_TILES,       // scan tiles of the key space
     BM_LINKS,           // page links
-    BM_ZERO_CELLS,      // cell counters in 4 KiB pieces
+    BM_ZERO_CELLS,      // cell counters (and page flags) in 4 KiB pieces
     BM_CELL_TILES,      // scan tiles of the cell counters
     BM_CANON,
     BM_P2G,
@@ -171,6 +197,8 @@ struct BatchPlan {
 void batch_scene_ctas(int64_t n, uint32_t key_space, int nb_cap, int ng_cap, int sms, int real_bytes,
                       int ctas[kBatchMaps]);
 
+// The batch's scenes enter with their keys and page flags set by the G2P (or
+// key pass) that wrote their positions, as launch_binning with keys_ready.
 template <typename R>
 cudaError_t launch_batch_binning(const SceneArgs<R>* args, const BatchPlan& plan, cudaStream_t s);
 template <typename R>
@@ -179,6 +207,6 @@ template <typename R>
 cudaError_t launch_batch_grid(const SceneArgs<R>* args, const BatchPlan& plan, cudaStream_t s);
 template <typename R>
 cudaError_t launch_batch_g2p(const SceneArgs<R>* args, const BatchPlan& plan, cudaStream_t s);
-constexpr int kBatchLaunchesPerSubstep = 25;
+constexpr int kBatchLaunchesPerSubstep = 23;
 
 }  // namespace gmpm

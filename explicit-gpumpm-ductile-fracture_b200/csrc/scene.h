@@ -46,6 +46,10 @@ struct SceneBase {
     virtual int parity() const = 0;
     virtual int kernels_per_substep() const = 0;
     virtual gmpm_status launch_substep(cudaStream_t s, int parity) = 0;
+    // A key pass over the current positions on s, unless the last writer of
+    // the positions (a G2P or an earlier key pass) left their keys in place;
+    // substeps captured afterwards skip their key pass.
+    virtual gmpm_status ensure_keys(cudaStream_t s) = 0;
     // own_launches: the substeps ran the scene's own kernels (a branch or the
     // plain path), not a batch's launches over many scenes.
     virtual void commit_substeps(int n, bool own_launches = true) = 0;

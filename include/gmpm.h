@@ -446,7 +446,7 @@ gmpm_status gmpm_scene_load(gmpm_context* ctx, const char* path, gmpm_scene** ou
  * (Simulator.cpp:227-259).  A batch advances many independent scenes of uneven size, each with its
  * own grid, with one CUDA graph launch per substep.  Scenes whose kernels are of one kind (precision,
  * P2G mode, energy models, FP64 fallback) advance together with one launch per stage of the substep
- * over a device table of the scenes (25 launches per kind, whatever the number of scenes); scenes
+ * over a device table of the scenes (23 launches per kind, whatever the number of scenes); scenes
  * with the implicit phase field run their own launch sequences on parallel branches of the graph.
  * Each scene's results are the same as stepping it alone (bitwise in deterministic mode).  The
  * autotuner times candidate launch shapes (the share of SMs each scene's page- and slot-parallel
