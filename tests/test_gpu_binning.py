@@ -68,3 +68,21 @@ def test_duplicate_and_boundary_positions(pkg, ctx, oracle):
     gpu.rebin()
     orc = oracle.OracleScene(d, pos, mass)
     assert_same_binning(gpu, orc)
+
+
+@pytest.mark.parametrize("name", ["notched_bar", "plates32"])
+def test_binning_from_g2p_keys_bit_exact(pkg, ctx, oracle, name):
+    """A substep's binning starts from the cell keys its previous G2P formed
+    for the positions it wrote (no key pass): the binning the 25th substep
+    ran equals the oracle's binning of the positions the 24th wrote."""
+    G = pkg.gmpm
+    sp = SCENES[name](pkg.scenes)
+    gpu = sp.build(ctx)
+    gpu.substep(24)
+    pos = gpu.read("position", order=G.ORDER_INTERNAL)
+    mass = gpu.read("mass", order=G.ORDER_INTERNAL)
+    ids = gpu.read("id", order=G.ORDER_INTERNAL).astype(np.int64)
+    gpu.substep(1)
+    assert gpu.sync() == G.OK
+    orc = oracle.OracleScene(sp.desc, pos, mass, None, sp.material_ids[ids])
+    assert_same_binning(gpu, orc)
