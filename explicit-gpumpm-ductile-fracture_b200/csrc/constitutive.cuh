@@ -17,11 +17,16 @@ template <typename R> __device__ __forceinline__ R c_p23() { return R(2.0f / 3.0
 template <typename R> __device__ __forceinline__ R c_sqrt_p23() { return sqrt(R(2.0f / 3.0f)); }
 template <typename R> __device__ __forceinline__ R c_sqrt_p23_f() { return R(sqrtf(2.0f / 3.0f)); }
 
-__device__ __forceinline__ float exp_r(float x) { return expf(x); }
+// FP32 exponentials and powers on the special-function unit (__expf, __powf:
+// a few ulp for the small arguments here, the exponentials of strains and of
+// softening terms and J^(-2/3) with J near 1); FP64 and the FP32 logarithms
+// (Hencky strains and ln J near 1, where only a relative-accurate log keeps
+// the small strains) use the accurate library functions.
+__device__ __forceinline__ float exp_r(float x) { return __expf(x); }
 __device__ __forceinline__ double exp_r(double x) { return exp(x); }
 __device__ __forceinline__ float log_r(float x) { return logf(x); }
 __device__ __forceinline__ double log_r(double x) { return log(x); }
-__device__ __forceinline__ float pow_r(float x, float y) { return powf(x, y); }
+__device__ __forceinline__ float pow_r(float x, float y) { return __powf(x, y); }
 __device__ __forceinline__ double pow_r(double x, double y) { return pow(x, y); }
 
 template <typename R, typename MR>
@@ -29,7 +34,7 @@ __device__ __forceinline__ R hardening_R(const MaterialDev<MR>& m, R alpha) {
     const R y = R(m.yield_stress);
     if (m.hardening_law == GMPM_HARDENING_LINEAR) return y + R(m.hardening) * alpha;
     const R sq = c_sqrt_p23_f<R>();
-    return sq * y - (sq * y - y) / exp_r(R(m.hardening) * alpha);
+    return sq * y - div_r(sq * y - y, exp_r(R(m.hardening) * alpha));
 }
 
 template <typename R>
@@ -55,7 +60,7 @@ __device__ __forceinline__ void svd_of(const R* Fin, R* U, R* S, R* V, StressOut
     o.svd_ok = svd3(A, U, S, V);
     const R smax = fmax(fabs(S[0]), fmax(fabs(S[1]), fabs(S[2])));
     const R smin = fmin(fabs(S[0]), fmin(fabs(S[1]), fabs(S[2])));
-    o.smin_over_smax = (smax > R(0)) ? smin / smax : R(0);
+    o.smin_over_smax = (smax > R(0)) ? div_r(smin, smax) : R(0);
 }
 
 template <typename R, typename MR>
@@ -72,7 +77,7 @@ __device__ __forceinline__ void von_mises_from_svd(const MaterialDev<MR>& m, R V
     tt[2] = C1 * eps[0] + C1 * eps[1] + C0 * eps[2];
     const R ttF = sqrt(tt[0] * tt[0] + tt[1] * tt[1] + tt[2] * tt[2]);
     const R tsum = tt[0] + tt[1] + tt[2];
-    const R divider = tsum / R(3);
+    const R divider = div_r(tsum, R(3));
     R tdev[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) tdev[k] = g * (tt[k] - divider);
@@ -86,7 +91,7 @@ __device__ __forceinline__ void von_mises_from_svd(const MaterialDev<MR>& m, R V
     if (y >= R(1e-12)) {
         R dl = R(0);
         const R bss = p23 * g * tsum;
-        if (bss > R(0)) dl = y / bss;
+        if (bss > R(0)) dl = div_r(y, bss);
         if (dl > R(m.dlambda_cap)) dl = R(m.dlambda_cap);
         if (alpha < R(m.alpha_cap)) {
             alpha += sp23 * dl;
@@ -98,7 +103,7 @@ __device__ __forceinline__ void von_mises_from_svd(const MaterialDev<MR>& m, R V
         // yield test uses the full trial stress, so a hydrostatic trial state
         // (equal singular values, exact in FP32) can yield with tau_dev = 0.
         // There is no deviator to scale then: the factor is 0 instead of NaN.
-        const R taudiv = tn > R(0) ? (R(1) / tn) * p23 * g * tsum * dl : R(0);
+        const R taudiv = tn > R(0) ? div_r(R(1), tn) * p23 * g * tsum * dl : R(0);
         const R p2 = (R(1) / R(3)) * tsum;
         R tnn[3];
 #pragma unroll
@@ -111,7 +116,7 @@ __device__ __forceinline__ void von_mises_from_svd(const MaterialDev<MR>& m, R V
         const R cap = R(m.strain_cap);
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-            if (en[k] > cap) en[k] = en[k] * (cap / nS);
+            if (en[k] > cap) en[k] = en[k] * div_r(cap, nS);
 #pragma unroll
         for (int k = 0; k < 3; ++k) S[k] = exp_r(en[k]);
         // F = U diag(S) V^T (column-major output)
@@ -141,7 +146,7 @@ __device__ __forceinline__ void von_mises_from_svd(const MaterialDev<MR>& m, R V
         Gc = R(m.fracture_energy) *
              (((R(1) - R(m.residual_fracture)) * exp_r(R(m.softening_onset) - p)) + R(m.residual_fracture));
     const R theta = R(m.theta), one_minus_theta = R(m.one_minus_theta);
-    o.FP = R(4) * R(m.length_scale) * one_minus_theta * psi * (R(1) / Gc) + R(1);
+    o.FP = R(4) * R(m.length_scale) * one_minus_theta * psi * div_r(R(1), Gc) + R(1);
     const R tvol = (kappa * R(0.5)) * (J * J - R(1));
     const R third = (R(1) / R(3)) * bbs;
     const R gn = c * c * one_minus_theta + theta;

@@ -22,6 +22,14 @@ template <> struct SvdEps<double> {
 __device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrt_r(double x) { return 1.0 / sqrt(x); }
 
+// Quotients: in FP32 the reciprocal-based __fdividef (within 2 ulp for the
+// normal-range divisors met here: singular values, stress norms, material
+// constants), in FP64 IEEE division as in the oracle.  An IEEE FP32 division
+// is a multi-instruction sequence with a slow-path branch; the SVD and return
+// map take about a dozen per particle.
+__device__ __forceinline__ float div_r(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double div_r(double a, double b) { return a / b; }
+
 // Conventional Givens: [c -s; s c][a; b] = [*; 0]  (givens.hpp:48-59)
 template <typename R>
 __device__ __forceinline__ void givens_conventional(R a, R b, R& c, R& s) {
@@ -116,8 +124,14 @@ __device__ __forceinline__ void process_block(const R* B, R* U, R* S, R* V) {
     R uc, us;
     {
         const R x0 = a00 + a11, x1 = a10 - a01;
-        const R d = sqrt(x0 * x0 + x1 * x1);
-        if (d != R(0)) {
+        const R d2 = x0 * x0 + x1 * x1;
+        if (sizeof(R) == 4 && d2 >= R(FLT_MIN)) {
+            // FP32: one reciprocal square root for both quotients
+            const R id = rsqrt_r(d2);
+            uc = x0 * id;
+            us = -x1 * id;
+        } else if (d2 != R(0)) {
+            const R d = sqrt(d2);
             uc = x0 / d;
             us = -x1 / d;
         } else {
@@ -139,7 +153,7 @@ __device__ __forceinline__ void process_block(const R* B, R* U, R* S, R* V) {
     } else {
         const R tau = R(0.5) * (x - z);
         const R w = sqrt(tau * tau + y2);
-        const R t = (tau > R(0)) ? y / (tau + w) : y / (tau - w);
+        const R t = div_r(y, (tau > R(0)) ? (tau + w) : (tau - w));
         cosine = rsqrt_r(t * t + R(1));
         sine = -t * cosine;
         const R c2 = cosine * cosine, csy2 = R(2) * cosine * sine * y, s2 = sine * sine;
@@ -256,7 +270,7 @@ __device__ __forceinline__ bool svd3(const R* A, R* U, R* S, R* V, int max_sweep
         const R wa1 = a1 * a1 + b0 * b0, wa2 = a2 * a2 + b1 * b1;
         const R d = R(0.5) * (wa1 - wa2);
         const R bs = g1 * g1;
-        const R mu = wa2 - copysign(bs / (fabs(d) + sqrt(d * d + bs)), d);
+        const R mu = wa2 - copysign(div_r(bs, fabs(d) + sqrt(d * d + bs)), d);
         R c, s;
         givens_conventional(a0 * a0 - mu, g0, c, s);
         rot_cols<0, 1>(B, c, s);
