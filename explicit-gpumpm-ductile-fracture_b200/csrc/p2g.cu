@@ -52,8 +52,9 @@ template <typename R> struct P2GChunk;
 template <> struct P2GChunk<float> { static constexpr int value = 512; };
 template <> struct P2GChunk<double> { static constexpr int value = 256; };
 
-// Record layout: 8 common words, then one 12-word block per channel group g
-// at RF_BLOCK + 12 g:
+// Record layout: 8 common words (the x and y offsets from the base node in
+// cells, xp/dx; the three z weights and their gradients), then one 12-word
+// block per channel group g at RF_BLOCK + 12 g:
 //   U, A0, A1, A2 | S0, S1, S2, s1 | t0, t1, t2, t3
 // with, for a lane of stencil column (i, j) and node k of the sweep,
 //   momentum_g += w (U + A0 i + A1 j + A2 k) + (S0 gxy0 + S1 gxy1) wz + S2 wxy gz
@@ -121,8 +122,9 @@ __device__ __forceinline__ void build_record(const SceneDev<R>* __restrict__ sc,
 #pragma unroll
     for (int a = 0; a < 3; ++a) xp[a] = raw[RW_X + a] - R(base[a]) * dx;
     R out[kRec];
-    out[RF_XP0] = xp[0];
-    out[RF_XP1] = xp[1];
+    // x and y offsets in cells: the product every lane's weight needs, formed once
+    out[RF_XP0] = xp[0] * inv_dx;
+    out[RF_XP1] = xp[1] * inv_dx;
     bspline1d(xp[2], inv_dx, out + RF_WZ, out + RF_GZ);
     const R m = raw[RW_M];
     const R V = raw[RW_VOL];
@@ -198,13 +200,13 @@ __device__ __forceinline__ void load_words(const R* __restrict__ src, R* dst) {
 // One particle of cell z-index CZ into a lane's 6 z-nodes x 3 channels.
 template <int CZ, typename R>
 __device__ __forceinline__ void accumulate(const R* __restrict__ rec, int g, const Piece<R>& px, const Piece<R>& py,
-                                           R inv_dx, R fi, R fj, R* acc) {
+                                           R fi, R fj, R* acc) {
     R cw[8], bw[12];
     load_words<8>(rec, cw);
     load_words<12>(rec + RF_BLOCK + 12 * g, bw);
     R wx, gx, wy, gy;
-    px.eval(cw[RF_XP0] * inv_dx, wx, gx);
-    py.eval(cw[RF_XP1] * inv_dx, wy, gy);
+    px.eval(cw[RF_XP0], wx, gx);
+    py.eval(cw[RF_XP1], wy, gy);
     const R wxy = wx * wy, gxy0 = gx * wy, gxy1 = wx * gy;
     const R al = bw[4] * gxy0 + bw[5] * gxy1, be = bw[6] * wxy;
     const R s1w = bw[7] * wxy;
@@ -226,11 +228,11 @@ __device__ __forceinline__ void accumulate(const R* __restrict__ rec, int g, con
 
 template <int CZ, typename R>
 __device__ __forceinline__ void sweep_cell(const R* __restrict__ recs, const int* __restrict__ s_cs, int cb, int c0,
-                                           int c1, int g, const Piece<R>& px, const Piece<R>& py, R inv_dx, R fi,
-                                           R fj, R* acc) {
+                                           int c1, int g, const Piece<R>& px, const Piece<R>& py, R fi, R fj,
+                                           R* acc) {
     const int lo = max(s_cs[cb + CZ], c0) - c0, hi = min(s_cs[cb + CZ + 1], c1) - c0;
 #pragma unroll 4
-    for (int p = lo; p < hi; ++p) accumulate<CZ>(recs + (size_t)p * kRec, g, px, py, inv_dx, fi, fj, acc);
+    for (int p = lo; p < hi; ++p) accumulate<CZ>(recs + (size_t)p * kRec, g, px, py, fi, fj, acc);
 }
 
 // Channel of slot q (0..2) of group g's accumulator row.
@@ -481,10 +483,10 @@ __device__ __forceinline__ void p2g_body(VB vb, const SceneDev<R>* __restrict__ 
         {
             const int* s_cs = S.cs[m0];
             const int c1 = c0 + n0;
-            sweep_cell<0>(recs, s_cs, cb, c0, c1, g, px, py, inv_dx, fi, fj, acc);
-            sweep_cell<1>(recs, s_cs, cb, c0, c1, g, px, py, inv_dx, fi, fj, acc);
-            sweep_cell<2>(recs, s_cs, cb, c0, c1, g, px, py, inv_dx, fi, fj, acc);
-            sweep_cell<3>(recs, s_cs, cb, c0, c1, g, px, py, inv_dx, fi, fj, acc);
+            sweep_cell<0>(recs, s_cs, cb, c0, c1, g, px, py, fi, fj, acc);
+            sweep_cell<1>(recs, s_cs, cb, c0, c1, g, px, py, fi, fj, acc);
+            sweep_cell<2>(recs, s_cs, cb, c0, c1, g, px, py, fi, fj, acc);
+            sweep_cell<3>(recs, s_cs, cb, c0, c1, g, px, py, fi, fj, acc);
         }
         if (!last0) continue;
 
