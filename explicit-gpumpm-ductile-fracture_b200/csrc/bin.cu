@@ -26,6 +26,10 @@ constexpr int kBinILP = 4;
 // The kernels' bodies take the CTA's index within its scene's share of the
 // launch (VB, common.cuh); the __global__ wrappers below each body serve a
 // one-scene launch, the batched launches at the end of this file many scenes.
+
+// The key pass: cell keys and page flags of positions that no G2P wrote
+// (creation, restore, rebin).  A substep's binning starts from the keys its
+// previous G2P formed for the positions it wrote.
 template <typename R>
 __device__ __forceinline__ void bin_keys_body(VB vb, int64_t n, const R* __restrict__ x0, const R* __restrict__ x1,
                                               const R* __restrict__ x2, const SceneDev<R>* __restrict__ sc,
