@@ -73,6 +73,15 @@ def measured_peaks() -> dict:
     return dict(hbm_gbs=6650.0, source="fallback")
 
 
+def clocks_median_mhz(clocks) -> float | None:
+    """Median SM clock sampled during the timed region, if any."""
+    try:
+        v = clocks.summary().get("sm_mhz")
+        return float(v) if v else None
+    except Exception:
+        return None
+
+
 def measured_traffic() -> dict:
     """DRAM bytes per particle per kernel from the committed ncu summary, if any."""
     p = ROOT / "profiles" / "traffic_per_particle.json"
@@ -288,6 +297,22 @@ def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
                           frac=round(gbs / peaks["hbm_gbs"], 4),
                           traffic=(int(tr * sp.n) if tr is not None else None))
     dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    # Issue roofline of the transfer kernels: warp instructions per particle (ncu,
+    # the committed profile) x particles / (SMs x 4 schedulers x SM clock).  P2G
+    # and G2P are bound by issue and latency, not by HBM, so this is the ceiling
+    # that explains their time.
+    issue = {}
+    ipp = traffic.get("warp_instructions_per_particle", {})
+    props = torch.cuda.get_device_properties(dev)
+    sm_hz = 1e6 * (clocks_median_mhz(clocks) or 1965.0)
+    peak_ips = props.multi_processor_count * 4 * sm_hz
+    for k in ("p2g", "g2p"):
+        if k in ipp and kernels[k]["ms"] > 0:
+            bound_ms = 1e3 * ipp[k] * sp.n / peak_ips
+            issue[k] = dict(warp_instructions_per_particle=ipp[k], bound_ms=round(bound_ms, 4),
+                            achieved=round(ipp[k] * sp.n / (kernels[k]["ms"] / 1e3) / 1e12, 4),
+                            peak=round(peak_ips / 1e12, 4), unit="warp instr/ns",
+                            frac=round(bound_ms / kernels[k]["ms"], 4))
 
     # end to end through the C-ABI, the reference's frame loop: host-set velocity
     # conditions (H2D), one substep, positions + damage back to pinned host memory (D2H).
@@ -337,7 +362,7 @@ def run_ours(args, pkg, rank: int, local_rank: int, world: int, dist):
                         "copies the same two fields as FP64 plus a colour word, 36 B/particle); reads "
                         "overlapped with the next substep (gmpm_read_particles_async, all landed at the end); "
                         "blocking_value: the same loop with gmpm_read_particles")
-    return dict(sp=sp, what=what, value=value, ms_max=ms_max, launches=launches, clocks=clocks.summary(),
+    return dict(sp=sp, what=what, value=value, ms_max=ms_max, launches=launches, clocks=clocks.summary(), issue=issue,
                 kernels=kernels, dom=dom, peaks=peaks, e2e=e2e, status=status, build_s=build_s, diag=diag)
 
 
@@ -598,7 +623,7 @@ def main():
             roofline=dict(bound="hbm", kernel=res["dom"], achieved=k["achieved_gbs"], peak=res["peaks"]["hbm_gbs"],
                           unit="GB/s", frac=k["frac"], traffic=k["traffic"],
                           peak_source=res["peaks"]["source"]),
-            kernels=res["kernels"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
+            issue_roofline=res["issue"], kernels=res["kernels"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
             gpu_launches=res["launches"], status=pkg.gmpm.STATUS_NAMES.get(res["status"], res["status"]),
             n_blocks=res["diag"]["n_blocks"], n_grid_blocks=res["diag"]["n_grid_blocks"], batched=batched, served=served,
             served_sustainable=sustainable)
