@@ -364,9 +364,8 @@ const char* gmpm_status_string(gmpm_status status);
  * every GPU loading the library holds until process exit.  All calls share
  * it: calls that overlap on the GPU (different streams, or threads without
  * ordering) race and must be serialised by the caller.  The first call on a
- * device resolves the array's address with cudaGetSymbolAddress; make that
- * first call before any stream capture.  The returned status is that of this
- * call's own API calls and launches. */
+ * device resolves the array's address with cudaGetSymbolAddress.  The returned
+ * status is that of this call's own API calls and launches. */
 #define GMPM_NOALLOC_MAX_PARTICLES 1048576
 #define GMPM_NOALLOC_MAX_RES 128
 #define GMPM_NOALLOC_SCRATCH_BYTES 21269248
