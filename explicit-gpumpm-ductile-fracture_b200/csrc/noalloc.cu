@@ -53,34 +53,19 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 __global__ void k_compact_keys(uint32_t key_space, const uint8_t* __restrict__ flag, const int32_t* __restrict__ rank,
                                uint32_t* __restrict__ out, int cap, Counters* cnt);
 
-// Page/cell keys of interleaved xyz positions: the same FP64 arithmetic as
-// the scene binning (cal_cellId, Particle_kernal.cu:158-165).
+// Page/cell keys of interleaved xyz positions: the scene binning's cell_key
+// (common.cuh; cal_cellId, Particle_kernal.cu:158-165).
 __global__ void k_noalloc_keys(int64_t n, const float* __restrict__ pos, double inv_dx, int rx, int ry, int rz,
                                uint32_t* __restrict__ keys, uint8_t* __restrict__ page_flag, Counters* cnt) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int res[3] = {rx, ry, rz};
-    int base[3];
+    const float x[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
     bool bad = false;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const double t = __dadd_rn(__dmul_rn((double)pos[3 * i + a], inv_dx), 0.5);
-        const int hi = res[a] - 3;
-        if (!(t >= 1.0)) {
-            base[a] = 0;
-            bad = true;
-        } else if (t >= (double)(hi + 2)) {
-            base[a] = hi;
-            bad = true;
-        } else {
-            base[a] = (int)t - 1;
-        }
-    }
+    const uint32_t key = cell_key(x, inv_dx, res, bad);
     if (bad) raise_flag(cnt, GMPM_FLAG_OUT_OF_DOMAIN);
-    const uint32_t cell = (uint32_t)(((base[0] & 3) << 4) | ((base[1] & 3) << 2) | (base[2] & 3));
-    const uint32_t pk = page_key(base[0] >> 2, base[1] >> 2, base[2] >> 2);
-    keys[i] = (pk << 6) | cell;
-    page_flag[pk] = 1;
+    keys[i] = key;
+    page_flag[key >> 6] = 1;
 }
 
 namespace {
