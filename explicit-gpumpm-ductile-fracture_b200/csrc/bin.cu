@@ -354,7 +354,9 @@ cudaError_t launch_binning(const SceneDev<R>* sc, const PState<R>& st, BinDev bi
     const int64_t ncell = (int64_t)bin.nb_cap * 64;
     cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), stream);
     launch_bin_hist(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap, stream);
-    scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, ncell, bin.cell_start + ncell, scan, stream);
+    // the cells of the active pages only (the page scan above counted them)
+    scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, ncell, bin.cell_start + ncell, scan, stream,
+                            &cnt->n_blocks);
     cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), stream);
     launch_bin_scatter(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, bin.perm, bin.keys_sorted,
                        bin.nb_cap, stream);
@@ -438,6 +440,7 @@ struct ScanSel<0> {
     static __device__ int64_t n(const BinDev& b) { return b.key_space; }
     static __device__ int32_t* out(const BinDev& b) { return b.page_rank; }
     static __device__ int32_t* total(const BinDev& b, Counters* c) { return &c->n_blocks; }
+    static __device__ const int32_t* live(Counters*) { return nullptr; }
 };
 template <>
 struct ScanSel<1> {
@@ -446,6 +449,7 @@ struct ScanSel<1> {
     static __device__ int64_t n(const BinDev& b) { return b.key_space; }
     static __device__ int32_t* out(const BinDev& b) { return b.grid_rank; }
     static __device__ int32_t* total(const BinDev& b, Counters* c) { return &c->n_grid_blocks; }
+    static __device__ const int32_t* live(Counters*) { return nullptr; }
 };
 template <>
 struct ScanSel<2> {
@@ -454,6 +458,7 @@ struct ScanSel<2> {
     static __device__ int64_t n(const BinDev& b) { return (int64_t)b.nb_cap * 64; }
     static __device__ int32_t* out(const BinDev& b) { return b.cell_start; }
     static __device__ int32_t* total(const BinDev& b, Counters*) { return b.cell_start + (int64_t)b.nb_cap * 64; }
+    static __device__ const int32_t* live(Counters* c) { return &c->n_blocks; }  // the active pages' cells
 };
 
 template <typename R, int kWhich>
@@ -462,7 +467,7 @@ __global__ void __launch_bounds__(kScanThreads) k_batch_scan_reduce(const SceneA
     VB vb;
     const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
     using S = ScanSel<kWhich>;
-    scan_reduce_body(vb, S::in(a.bin), S::n(a.bin), a.scan.tile_sums);
+    scan_reduce_body(vb, S::in(a.bin), S::n(a.bin), a.scan.tile_sums, S::live(a.cnt));
 }
 
 template <typename R, int kWhich>
@@ -481,7 +486,7 @@ __global__ void __launch_bounds__(kScanThreads) k_batch_scan_apply(const SceneAr
     VB vb;
     const SceneArgs<R>& a = A[scene_of_block(start, ns, vb)];
     using S = ScanSel<kWhich>;
-    scan_apply_body(vb, S::in(a.bin), S::n(a.bin), a.scan.tile_sums, S::out(a.bin));
+    scan_apply_body(vb, S::in(a.bin), S::n(a.bin), a.scan.tile_sums, S::out(a.bin), S::live(a.cnt));
 }
 
 template <typename R>

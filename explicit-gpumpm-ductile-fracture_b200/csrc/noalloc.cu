@@ -145,7 +145,9 @@ extern "C" gmpm_status gmpm_bin_positions_noalloc(const float* positions, int64_
         e = launch_kernel(k_compact_keys, dim3(gk), dim3(T), 0, s, kNoAllocKeySpace, (const uint8_t*)bin.page_flag,
                           (const int32_t*)bin.page_rank, bin.block_keys, (int)bin.nb_cap, cnt);
     if (e == cudaSuccess) e = launch_bin_hist(n, bin.keys, bin.page_rank, bin.cell_count, bin.nb_cap, s);
-    if (e == cudaSuccess) e = scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, ncell, bin.cell_start + ncell, scan, s);
+    if (e == cudaSuccess)
+        e = scan_exclusive<int32_t>(bin.cell_count, bin.cell_start, ncell, bin.cell_start + ncell, scan, s,
+                                    &cnt->n_blocks);
     if (e == cudaSuccess) e = cudaMemsetAsync(bin.cell_count, 0, ncell * sizeof(int32_t), s);
     if (e == cudaSuccess)
         e = launch_bin_scatter(n, bin.keys, bin.page_rank, bin.cell_start, bin.cell_count, perm, keys_sorted,

@@ -56,14 +56,28 @@ __device__ __forceinline__ int32_t block_exclusive_sum(int32_t x, int32_t* total
     return r;
 }
 
+// Entries scanned: all n, or with `live` (a device count of live blocks of 64
+// entries, the active pages of a cell scan, whose capacity is larger) only the
+// live entries.  The scan then writes the live entries and the one after them,
+// which receives the total; the entries beyond are left as they are, and no
+// reader looks past the live pages.
+__device__ __forceinline__ int64_t scan_live_len(int64_t n, const int32_t* live) {
+    return live ? min(n, (int64_t)max(*live, 0) * 64) : n;
+}
+
 // Bodies take the CTA's tile index within its scene's scan (VB, common.cuh),
 // so that the same code serves one-scene and batched launches.
 template <typename TIn>
 __device__ __forceinline__ void scan_reduce_body(VB vb, const TIn* __restrict__ in, int64_t n,
-                                                 int32_t* __restrict__ tile_sums) {
+                                                 int32_t* __restrict__ tile_sums, const int32_t* live = nullptr) {
+    const int64_t m = scan_live_len(n, live);
+    if ((int64_t)vb.b * kScanTile >= m) {  // a tile past the live entries (whole CTA)
+        if (threadIdx.x == 0) tile_sums[vb.b] = 0;
+        return;
+    }
     const int64_t base = (int64_t)vb.b * kScanTile + (int64_t)threadIdx.x * kScanItems;
     int32_t v[kScanItems];
-    scan_load(in, n, base, v);
+    scan_load(in, m, base, v);
     int32_t s = 0;
 #pragma unroll
     for (int q = 0; q < kScanItems; ++q) s += v[q];
@@ -74,8 +88,9 @@ __device__ __forceinline__ void scan_reduce_body(VB vb, const TIn* __restrict__ 
 
 template <typename TIn>
 __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const TIn* __restrict__ in, int64_t n,
-                                                               int32_t* __restrict__ tile_sums) {
-    scan_reduce_body(own_blocks(), in, n, tile_sums);
+                                                               int32_t* __restrict__ tile_sums,
+                                                               const int32_t* __restrict__ live) {
+    scan_reduce_body(own_blocks(), in, n, tile_sums, live);
 }
 
 // Single CTA: exclusive scan of the tile sums in place, total to *total.
@@ -109,10 +124,14 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t* __r
 
 template <typename TIn>
 __device__ __forceinline__ void scan_apply_body(VB vb, const TIn* __restrict__ in, int64_t n,
-                                                const int32_t* __restrict__ tile_offsets, int32_t* __restrict__ out) {
+                                                const int32_t* __restrict__ tile_offsets, int32_t* __restrict__ out,
+                                                const int32_t* live = nullptr) {
+    const int64_t m = scan_live_len(n, live);
+    const int64_t w = min(n, m + 1);  // entries written: the live ones and the total after them
+    if ((int64_t)vb.b * kScanTile >= w) return;  // whole CTA
     const int64_t base = (int64_t)vb.b * kScanTile + (int64_t)threadIdx.x * kScanItems;
     int32_t v[kScanItems];
-    scan_load(in, n, base, v);
+    scan_load(in, m, base, v);
     int32_t s = 0;
 #pragma unroll
     for (int q = 0; q < kScanItems; ++q) s += v[q];
@@ -120,7 +139,7 @@ __device__ __forceinline__ void scan_apply_body(VB vb, const TIn* __restrict__ i
     int32_t run = block_exclusive_sum(s, &tot) + tile_offsets[vb.b];
 #pragma unroll
     for (int q = 0; q < kScanItems; ++q) {
-        if (base + q < n) out[base + q] = run;
+        if (base + q < w) out[base + q] = run;
         run += v[q];
     }
 }
@@ -128,22 +147,24 @@ __device__ __forceinline__ void scan_apply_body(VB vb, const TIn* __restrict__ i
 template <typename TIn>
 __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const TIn* __restrict__ in, int64_t n,
                                                               const int32_t* __restrict__ tile_offsets,
-                                                              int32_t* __restrict__ out) {
-    scan_apply_body(own_blocks(), in, n, tile_offsets, out);
+                                                              int32_t* __restrict__ out,
+                                                              const int32_t* __restrict__ live) {
+    scan_apply_body(own_blocks(), in, n, tile_offsets, out, live);
 }
 
-// out[i] = sum_{j<i} in[j] for i < n; *total = sum of all.  Returns the
-// status of its own launches.
+// out[i] = sum_{j<i} in[j] for i < n; *total = sum of all.  With `live` (see
+// scan_live_len) only the live entries are read and the live entries and the
+// one after them written.  Returns the status of its own launches.
 template <typename TIn>
 inline cudaError_t scan_exclusive(const TIn* in, int32_t* out, int64_t n, int32_t* total, ScanScratch s,
-                                  cudaStream_t stream) {
+                                  cudaStream_t stream, const int32_t* live = nullptr) {
     const int64_t ntiles = (n + kScanTile - 1) / kScanTile;
     cudaError_t e = launch_kernel(k_scan_reduce<TIn>, dim3((unsigned)ntiles), dim3(kScanThreads), 0, stream, in, n,
-                                  s.tile_sums);
+                                  s.tile_sums, live);
     if (e == cudaSuccess) e = launch_kernel(k_scan_tiles, dim3(1), dim3(kScanThreads), 0, stream, s.tile_sums, ntiles, total);
     if (e == cudaSuccess)
         e = launch_kernel(k_scan_apply<TIn>, dim3((unsigned)ntiles), dim3(kScanThreads), 0, stream, in, n,
-                          (const int32_t*)s.tile_sums, out);
+                          (const int32_t*)s.tile_sums, out, live);
     return e;
 }
 
