@@ -86,3 +86,30 @@ def test_binning_from_g2p_keys_bit_exact(pkg, ctx, oracle, name):
     assert gpu.sync() == G.OK
     orc = oracle.OracleScene(sp.desc, pos, mass, None, sp.material_ids[ids])
     assert_same_binning(gpu, orc)
+
+
+def test_crowded_page_and_cell(pkg, ctx, oracle):
+    """Canonical order where the warp's buffer does not hold the page: a page of
+    1,280 particles (20 in each of its 64 cells, ranked in windows of whole
+    cells) and one cell of 1,000 particles (ranked from global memory), all
+    in shuffled order, bin exactly like the oracle's stable sort."""
+    G = pkg.gmpm
+    dx = 1.0 / 64
+    rng = np.random.default_rng(11)
+    # base node b for x = (b + 1 + u) dx, u in [-0.5, 0.5)
+    page = np.stack(np.meshgrid(np.arange(8, 12), np.arange(8, 12), np.arange(8, 12), indexing="ij"), -1).reshape(-1, 3)
+    crowded = np.repeat(page, 20, axis=0)
+    cell = np.repeat(np.array([[20, 20, 20]]), 1000, axis=0)
+    other = rng.integers(4, 56, size=(3000, 3))
+    base = np.concatenate([crowded, cell, other])
+    pos = (base + 1 + rng.random(base.shape) - 0.5) * dx
+    pos = pos[rng.permutation(len(pos))].astype(np.float32).astype(np.float64)
+    d = G.reference_defaults(dx, (64, 64, 64))
+    mass = np.full(len(pos), 1e-6)
+    gpu = G.Scene(ctx, d, pos, mass)
+    gpu.rebin()
+    assert gpu.sync() == G.OK
+    orc = oracle.OracleScene(d, pos, mass)
+    assert_same_binning(gpu, orc)
+    counts = np.diff(gpu.binning("cell_start"))
+    assert counts.max() >= 1000 and (counts >= 20).sum() >= 64
