@@ -138,9 +138,9 @@ def hexline(vals) -> str:
     return " ".join(float(v).hex() for v in vals)
 
 
-# Materials (E, nu) and grid spacings of the constitutive cases: the BASELINE
-# bar material, the reference's own scene material (Simulator.cpp:114-116) and
-# the plate extremes.
+# Materials (E, nu) and grid spacings of the constitutive cases: the notched
+# bar's material, the reference's own scene material (Simulator.cpp:114-116)
+# and the extremes of the plates' drawn stiffness.
 VM_MATERIALS = [(1e5, 0.3), (2e2, 0.4), (5e4, 0.25), (5e5, 0.3)]
 VM_DX = [1.0 / 256, 1.0 / 128]
 
