@@ -21,7 +21,7 @@ namespace gmpm {
 // kBinILP particles one CTA width apart (coalesced per round) and issues all
 // their loads before using any, so more requests are in flight per SM.
 constexpr int kBinThreads = 256;
-constexpr int kBinILP = 4;
+constexpr int kBinILP = 8;
 
 // The kernels' bodies take the CTA's index within its scene's share of the
 // launch (VB, common.cuh); the __global__ wrappers below each body serve a
